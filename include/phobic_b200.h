@@ -1,0 +1,204 @@
+/*
+ * phobic_b200.h -- C ABI of the B200 PHOBIC minimal-perfect-hash construction engine.
+ *
+ * The reference (stefanfred/PHOBIC-GPU) builds an MPHF with
+ *     MPHFbuilder::build(const std::vector<keyType>&, Mphf&)   include/phobicGpu/mphf_builder.h:47-48,315-321
+ * which hashes the keys on the host (mphf_builder.h:201-216), runs seven Vulkan
+ * compute stages (mphf_builder.h:137-199) and hands two arrays to the encoders
+ * through Mphf::setData (mphf.hpp:65-75):
+ *     pilots[buckets * partitions]      bucket-major, pilots[b * partitions + p]  (search.comp:170-174)
+ *     partition_offsets[partitions + 1] exclusive prefix of partition sizes, [0] = 0 (mphf_builder.h:254-257)
+ * This ABI replaces the host hash, the Vulkan runtime and the seven stages: it takes
+ * keys and returns exactly those two arrays.  The C++ layer (phobic_gpu_mphf.hpp in the
+ * package) keeps the reference's MPHFbuilder / MPHF / encoder surface on top of it.
+ *
+ * Conventions: plain pointers and sizes; every call returns a phobic_status; host or
+ * device buffers are named by flags; a context is used by one thread at a time.
+ */
+#ifndef PHOBIC_B200_H
+#define PHOBIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PHOBIC_API __attribute__((visibility("default")))
+#else
+#define PHOBIC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHOBIC_ABI_VERSION 1
+#define PHOBIC_FULCRUMS 2048 /* shaders/constants.glsl:1 */
+#define PHOBIC_MAX_BUCKET 256 /* sort_sum.comp bins: bucket sizes 1..256 */
+
+/* Status codes.  The reference throws std::runtime_error on Vulkan errors
+ * (include/app/check.h:7-25) and has undefined behaviour on overflow; here every
+ * condition is a code, and the C++ layer rethrows std::runtime_error. */
+typedef enum phobic_status {
+    PHOBIC_OK = 0,
+    PHOBIC_ERR_INVALID = 1,            /* bad argument, or a bucket id >= buckets from the fulcrum table */
+    PHOBIC_ERR_OOM = 2,                /* device or pinned-host allocation failed */
+    PHOBIC_ERR_BUCKET_OVERFLOW = 3,    /* a bucket of more than 256 keys */
+    PHOBIC_ERR_PARTITION_OVERFLOW = 4, /* a partition above max_partition_size keys */
+    PHOBIC_ERR_SEARCH_LIMIT = 5,       /* pilot counter reached its limit */
+    PHOBIC_ERR_TIMEOUT = 6,            /* a bounded wait expired */
+    PHOBIC_ERR_CUDA = 7,               /* CUDA runtime error (detail in phobic_last_error) */
+    PHOBIC_ERR_DUPLICATE_KEY = 8,      /* two keys of one bucket hash identically */
+    PHOBIC_ERR_BUDGET = 9,             /* request does not fit the server's memory budget */
+    PHOBIC_ERR_BUSY = 10,              /* server queue full */
+    PHOBIC_ERR_NO_DEVICE = 11,         /* no CUDA device / not sm_100 */
+    PHOBIC_ERR_NOT_FOUND = 12          /* unknown server ticket */
+} phobic_status;
+
+/* Key kinds (hasher.hpp:22-66). */
+typedef enum phobic_key_kind {
+    PHOBIC_KEYS_U64 = 0,       /* uint64_t[n], hashed as 8 little-endian bytes (xxhash::hash(uint64_t)) */
+    PHOBIC_KEYS_BYTES16 = 1,   /* 16-byte records hashed as 16 bytes (std::pair<u64,u64>, or Key under xxhash) */
+    PHOBIC_KEYS_PREHASHED = 2, /* 16-byte Key records used as-is (nohash, hasher.hpp:22-27) */
+    PHOBIC_KEYS_STRINGS = 3    /* ragged byte strings: data + offsets[n+1] (xxhash::hash(std::string)) */
+} phobic_key_kind;
+
+/* Construction parameters.  Derived on the host from MPHFconfig
+ * (mphf_config.h:26-64); phobic_config() computes them. */
+typedef struct phobic_params {
+    uint32_t partition_size;     /* P: expected keys per partition */
+    uint32_t buckets;            /* B: buckets per partition (1..65535) */
+    uint32_t max_partition_size; /* search bitmap capacity; 0 = 32*floor(1.5P/32) (search.comp:21) */
+    uint32_t max_pilot_counter;  /* cap on the pilot counter k; 0 = 1<<20 (also bounded by 2^31/ps) */
+    uint32_t fulcrums[PHOBIC_FULCRUMS]; /* bucket mapping table (mphf_config.h:44-55) */
+} phobic_params;
+
+typedef struct phobic_keys {
+    int32_t kind;            /* phobic_key_kind */
+    int32_t on_device;       /* 1: data/offsets are device pointers of the context's device */
+    uint64_t n;              /* number of keys (< 2^32, as mphf_builder.h:56) */
+    const void *data;        /* u64[n] | 16-byte records[n] | string bytes */
+    const uint64_t *offsets; /* strings only: offsets[n+1] into data */
+} phobic_keys;
+
+typedef struct phobic_result {
+    int32_t on_device;           /* 1: the two arrays are device pointers */
+    uint32_t *pilots;            /* [buckets * partitions], caller-allocated */
+    uint32_t *partition_offsets; /* [partitions + 1], caller-allocated */
+} phobic_result;
+
+/* Stage times in milliseconds, measured with CUDA events on the build stream.
+ * Labels follow the reference's HostTimer labels (mphf_builder.h:138-146, :229-290). */
+typedef struct phobic_timings {
+    float input_transfer;     /* host -> device copy of the keys (overlapped with bucket_sizes) */
+    float bucket_sizes;       /* hash + partition count (kernel K1) */
+    float partition_offsets;  /* decoupled-lookback scan (kernel K2) */
+    float key_redistribution; /* partition scatter (kernel K3) */
+    float search;             /* bucket sort + pilot search (kernel K4) */
+    float result_transfer;    /* device -> host copy of pilots and offsets */
+    float total;              /* first event to last event */
+    uint32_t kernels;         /* kernels launched by the call */
+} phobic_timings;
+
+typedef struct phobic_ctx phobic_ctx;
+typedef struct phobic_server phobic_server;
+
+/* ------------------------------------------------------------------ setup */
+
+/* Human-readable name of a status code. */
+PHOBIC_API const char *phobic_status_string(phobic_status s);
+
+/* Number of partitions for n keys: ceil(n / P) (mphf_builder.h:90). */
+PHOBIC_API uint32_t phobic_partitions(uint64_t n, uint32_t partition_size);
+
+/* MPHFconfig arithmetic (mphf_config.h:26-64, bucketers.h:20-50):
+ * bucketer 0 = OptBucketer (the default), 1 = UniformBucketer, 2 = SkewBucketer;
+ * bucketer_ctor != 0 selects MPHFconfig(Bucketer*, λ, P), which rounds P/λ instead of
+ * taking its ceiling.  Fills every field of *out (max_pilot_counter = 0). */
+PHOBIC_API phobic_status phobic_config(double lambda, uint32_t partition_size, int bucketer, int bucketer_ctor,
+                            phobic_params *out);
+
+/* Create a context on a CUDA device (one stream, pooled device buffers). */
+PHOBIC_API phobic_status phobic_ctx_create(int device, phobic_ctx **out);
+PHOBIC_API phobic_status phobic_ctx_destroy(phobic_ctx *ctx);
+/* Detail text of the last error on this context (never NULL). */
+PHOBIC_API const char *phobic_last_error(const phobic_ctx *ctx);
+/* Device bytes the context's pools hold now. */
+PHOBIC_API uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx);
+/* Device bytes one build of n keys needs (keys staging excluded when on_device). */
+PHOBIC_API uint64_t phobic_build_bytes_needed(const phobic_keys *keys, const phobic_params *params);
+
+/* ------------------------------------------------------------------ build
+ * Replaces BuildInvocation::run (mphf_builder.h:225-292) up to, not including,
+ * Mphf::setData.  Synchronous: returns when the result arrays are written. */
+PHOBIC_API phobic_status phobic_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                           const phobic_result *result, phobic_timings *timings);
+
+/* Convenience forms with host buffers (the reference's std::vector inputs). */
+PHOBIC_API phobic_status phobic_build_u64(phobic_ctx *ctx, const uint64_t *keys, uint64_t n, const phobic_params *params,
+                               uint32_t *pilots, uint32_t *partition_offsets, phobic_timings *timings);
+PHOBIC_API phobic_status phobic_build_strings(phobic_ctx *ctx, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                                   const phobic_params *params, uint32_t *pilots, uint32_t *partition_offsets,
+                                   phobic_timings *timings);
+
+/* ------------------------------------------------------------------ batch
+ * Many independent key sets built with one launch per stage: the partitions
+ * of all sets form one work list that the search kernel's CTAs share.
+ * results[i] receives set i; statuses[i] its status.  Returns the first error. */
+PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *sets, uint32_t nsets,
+                                 const phobic_params *params, const phobic_result *results,
+                                 phobic_status *statuses, phobic_timings *timings);
+
+/* ------------------------------------------------------------------ query
+ * MPHF::operator() (mphf.hpp:77-86) over the raw (unencoded) result arrays.
+ * positions[i] = slot of key i in [0, n_built).  Arrays may live on the host
+ * or the device (flags); positions follow keys->on_device. */
+PHOBIC_API phobic_status phobic_query(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                           uint32_t partitions, const phobic_result *built, uint32_t *positions);
+
+/* Bijection check (example.cpp:43-59) on the device: *bad = number of keys whose
+ * slot is out of range or already taken. */
+PHOBIC_API phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                            const phobic_result *built, uint64_t *bad);
+
+/* ------------------------------------------------------------------ debug
+ * Intermediates of one build for parity tests (host buffers, NULL to skip):
+ * keys4[4n] hashed Keys; bucket_sizes[partitions*buckets] (p-major). */
+PHOBIC_API phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                                 const phobic_result *result, uint32_t *keys4, uint32_t *bucket_sizes);
+
+/* ------------------------------------------------------------------ serving
+ * A build server: a request loop that admits key sets as they arrive against a
+ * device-memory budget, keeps buffers resident, overlaps admitted requests on
+ * several streams, and records per-request latency. */
+typedef struct phobic_server_config {
+    int32_t device;
+    uint32_t streams;        /* concurrent builds in flight (>= 1) */
+    uint32_t queue_capacity; /* pending requests before submit returns PHOBIC_ERR_BUSY */
+    uint64_t budget_bytes;   /* device memory the admitted builds may hold together */
+} phobic_server_config;
+
+typedef struct phobic_server_stats {
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t keys;
+    double p50_ms, p99_ms, max_ms; /* submit-to-completion latency */
+    double busy_ms;                /* wall time with at least one request in flight */
+    uint64_t peak_bytes;           /* largest admitted device footprint */
+} phobic_server_stats;
+
+PHOBIC_API phobic_status phobic_server_create(const phobic_server_config *cfg, phobic_server **out);
+/* Copies nothing: keys and result buffers must stay valid until the request completes. */
+PHOBIC_API phobic_status phobic_server_submit(phobic_server *srv, const phobic_keys *keys, const phobic_params *params,
+                                   const phobic_result *result, uint64_t *ticket);
+/* *done = 1 and *status set once the request finished. */
+PHOBIC_API phobic_status phobic_server_poll(phobic_server *srv, uint64_t ticket, int *done, phobic_status *status);
+/* Waits at most timeout_ms for the request (PHOBIC_ERR_TIMEOUT otherwise). */
+PHOBIC_API phobic_status phobic_server_wait(phobic_server *srv, uint64_t ticket, uint32_t timeout_ms, phobic_status *status);
+PHOBIC_API phobic_status phobic_server_drain(phobic_server *srv, uint32_t timeout_ms);
+PHOBIC_API phobic_status phobic_server_stats_get(phobic_server *srv, phobic_server_stats *out);
+PHOBIC_API phobic_status phobic_server_destroy(phobic_server *srv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHOBIC_B200_H */

@@ -1,0 +1,156 @@
+// C ABI entry points (include/phobic_b200.h).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "engine.hpp"
+#include "kernels.cuh"
+
+using namespace phobicb200;
+
+struct phobic_ctx {
+    Worker w;
+    std::string last_error;
+};
+
+extern "C" {
+
+const char *phobic_status_string(phobic_status s) {
+    switch (s) {
+    case PHOBIC_OK: return "ok";
+    case PHOBIC_ERR_INVALID: return "invalid argument";
+    case PHOBIC_ERR_OOM: return "out of memory";
+    case PHOBIC_ERR_BUCKET_OVERFLOW: return "bucket overflow (more than 256 keys)";
+    case PHOBIC_ERR_PARTITION_OVERFLOW: return "partition overflow";
+    case PHOBIC_ERR_SEARCH_LIMIT: return "pilot search limit reached";
+    case PHOBIC_ERR_TIMEOUT: return "timeout";
+    case PHOBIC_ERR_CUDA: return "cuda error";
+    case PHOBIC_ERR_DUPLICATE_KEY: return "duplicate keys";
+    case PHOBIC_ERR_BUDGET: return "request exceeds the memory budget";
+    case PHOBIC_ERR_BUSY: return "queue full";
+    case PHOBIC_ERR_NO_DEVICE: return "no suitable CUDA device";
+    case PHOBIC_ERR_NOT_FOUND: return "unknown ticket";
+    }
+    return "unknown status";
+}
+
+uint32_t phobic_partitions(uint64_t n, uint32_t partition_size) {
+    if (!partition_size) return 0;
+    return (uint32_t)((n + partition_size - 1) / partition_size);
+}
+
+// MPHFconfig (mphf_config.h:26-55) with the bucketers of bucketers.h:20-50.
+// This translation unit is compiled with -ffp-contract=off: every double
+// operation rounds on its own, so the table does not depend on FMA contraction.
+phobic_status phobic_config(double lambda, uint32_t partition_size, int bucketer, int bucketer_ctor,
+                            phobic_params *out) {
+    if (!out || !(lambda > 0.0) || partition_size == 0 || bucketer < 0 || bucketer > 2) return PHOBIC_ERR_INVALID;
+    double q = (double)partition_size / lambda;
+    double bq = bucketer_ctor ? std::round(q) : std::ceil(q);
+    if (!(bq >= 1.0) || bq > 65535.0) return PHOBIC_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    out->partition_size = partition_size;
+    out->buckets = (uint32_t)bq;
+    out->max_partition_size = default_max_partition(partition_size);
+    const double c = 0.2 * lambda / std::sqrt((double)partition_size);  // OptBucketer::init
+    const uint32_t top = out->buckets << 16;
+    out->fulcrums[0] = 0;
+    for (uint32_t xi = 1; xi < PHOBIC_FULCRUMS - 1; xi++) {
+        double x = (double)xi / (double)(PHOBIC_FULCRUMS - 1);
+        double y;
+        if (bucketer == 1) y = x;
+        else if (bucketer == 2) y = x < 0.6 ? x / 0.6 * 0.3 : 0.3 + (x - 0.6) / 0.4 * 0.7;
+        else y = (x + (1.0 - x) * std::log(1.0 - x)) * (1.0 - c) + c * x;
+        out->fulcrums[xi] = (uint32_t)(y * (double)top);
+    }
+    out->fulcrums[PHOBIC_FULCRUMS - 1] = top;
+    return PHOBIC_OK;
+}
+
+phobic_status phobic_ctx_create(int device, phobic_ctx **out) {
+    if (!out) return PHOBIC_ERR_INVALID;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return PHOBIC_ERR_NO_DEVICE;
+    }
+    phobic_ctx *c = new phobic_ctx();
+    std::string err;
+    phobic_status st = c->w.init(device, &err);
+    if (st != PHOBIC_OK) {
+        c->w.destroy();
+        delete c;
+        return st;
+    }
+    *out = c;
+    return PHOBIC_OK;
+}
+
+phobic_status phobic_ctx_destroy(phobic_ctx *ctx) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->w.destroy();
+    delete ctx;
+    return PHOBIC_OK;
+}
+
+const char *phobic_last_error(const phobic_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx) { return ctx ? ctx->w.arena.capacity() : 0; }
+
+uint64_t phobic_build_bytes_needed(const phobic_keys *keys, const phobic_params *params) {
+    if (!keys || !params || !params->partition_size) return 0;
+    return build_arena_bytes(keys, params, nullptr, false);
+}
+
+phobic_status phobic_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                           const phobic_result *result, phobic_timings *timings) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    phobic_status st = enqueue_build(ctx->w, keys, params, result, nullptr, &ctx->last_error);
+    if (st != PHOBIC_OK) return st;
+    return finish_build(ctx->w, timings, &ctx->last_error);
+}
+
+phobic_status phobic_build_u64(phobic_ctx *ctx, const uint64_t *keys, uint64_t n, const phobic_params *params,
+                               uint32_t *pilots, uint32_t *partition_offsets, phobic_timings *timings) {
+    phobic_keys k{PHOBIC_KEYS_U64, 0, n, keys, nullptr};
+    phobic_result r{0, pilots, partition_offsets};
+    return phobic_build(ctx, &k, params, &r, timings);
+}
+
+phobic_status phobic_build_strings(phobic_ctx *ctx, const uint8_t *bytes, const uint64_t *offsets, uint64_t n,
+                                   const phobic_params *params, uint32_t *pilots, uint32_t *partition_offsets,
+                                   phobic_timings *timings) {
+    phobic_keys k{PHOBIC_KEYS_STRINGS, 0, n, bytes, offsets};
+    phobic_result r{0, pilots, partition_offsets};
+    return phobic_build(ctx, &k, params, &r, timings);
+}
+
+phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                                 const phobic_result *result, uint32_t *keys4, uint32_t *bucket_sizes) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    DebugOut dbg{keys4, bucket_sizes};
+    phobic_status st = enqueue_build(ctx->w, keys, params, result, &dbg, &ctx->last_error);
+    if (st != PHOBIC_OK) return st;
+    return finish_build(ctx->w, nullptr, &ctx->last_error);
+}
+
+phobic_status phobic_query(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params, uint32_t partitions,
+                           const phobic_result *built, uint32_t *positions) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return run_query(ctx->w, keys, params, partitions, built, positions, nullptr, &ctx->last_error);
+}
+
+phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
+                            const phobic_result *built, uint64_t *bad) {
+    if (!ctx || !keys || !params || !bad) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    uint32_t partitions = phobic_partitions(keys->n, params->partition_size);
+    return run_query(ctx->w, keys, params, partitions, built, nullptr, bad, &ctx->last_error);
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+"""Seeded synthetic key sets for the build workloads.
+
+No public dataset is involved: every workload is generated from a seed.
+  * u64 keys: the splitmix64 stream (Vigna's public generator; state starts at the
+    seed, output i is the finalizer of seed + (i+1) * 0x9E3779B97F4A7C15).  It is
+    a bijection of the counter, so the keys are unique.
+  * strings: lengths uniform in [8, 64], bytes uniform over printable ASCII
+    (0x20..0x7E), duplicates replaced (only short strings can collide).
+  * batched sets: sizes log-uniform in [lo, hi].
+  * served stream: Poisson arrivals, sizes log-uniform, a u64/string mix.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+GAMMA = np.uint64(0x9E3779B97F4A7C15)
+M1 = np.uint64(0xBF58476D1CE4E5B9)
+M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(seed: int, n: int, start: int = 0, chunk: int = 1 << 24) -> np.ndarray:
+    out = np.empty(n, np.uint64)
+    with np.errstate(over="ignore"):
+        for lo in range(0, n, chunk):
+            hi = min(n, lo + chunk)
+            z = np.arange(start + lo + 1, start + hi + 1, dtype=np.uint64) * GAMMA + np.uint64(seed)
+            z = (z ^ (z >> np.uint64(30))) * M1
+            z = (z ^ (z >> np.uint64(27))) * M2
+            out[lo:hi] = z ^ (z >> np.uint64(31))
+    return out
+
+
+def strings(seed: int, n: int, min_len: int = 8, max_len: int = 64) -> tuple[np.ndarray, np.ndarray]:
+    """(bytes uint8[total], offsets uint64[n+1]) of n distinct printable strings."""
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(min_len, max_len + 1, n, dtype=np.int64)
+    offs = np.zeros(n + 1, np.uint64)
+    np.cumsum(lens, out=offs[1:])
+    data = rng.integers(0x20, 0x7F, int(offs[-1]), dtype=np.uint8)
+    # Strings of 8..10 bytes are the only ones with a non-negligible collision
+    # chance at these sizes; replace any repeat among them.
+    for L in range(min_len, min(max_len, 10) + 1):
+        idx = np.nonzero(lens == L)[0]
+        while idx.size:
+            rows = data[offs[idx].astype(np.int64)[:, None] + np.arange(L)]
+            _, first = np.unique(rows, axis=0, return_index=True)
+            dup = np.setdiff1d(np.arange(idx.size), first)
+            if not dup.size:
+                break
+            for d in idx[dup]:
+                s = int(offs[d])
+                data[s:s + L] = rng.integers(0x20, 0x7F, L, dtype=np.uint8)
+    return data, offs
+
+
+def set_sizes(seed: int, count: int, lo: int, hi: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), count))).astype(np.int64)
+
+
+def request_stream(seed: int, rate: float, seconds: float, lo: int, hi: int, string_frac: float):
+    """Arrival times (s), sizes and kinds ('u64' / 'strings') of a Poisson request stream."""
+    rng = np.random.default_rng(seed)
+    t, times = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            break
+        times.append(t)
+    k = len(times)
+    sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), k))).astype(np.int64)
+    kinds = np.where(rng.uniform(size=k) < string_frac, "strings", "u64")
+    return np.array(times), sizes, kinds

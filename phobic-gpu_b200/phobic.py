@@ -1,0 +1,351 @@
+"""Python binding of libphobic_b200.so (the C ABI in include/phobic_b200.h).
+
+Mirrors the reference's build surface (stefanfred/PHOBIC-GPU,
+include/phobicGpu/mphf_builder.h and mphf_config.h):
+
+    cfg = MPHFconfig(7.0, 2500)          # MPHFconfig(double λ, uint32_t P)
+    builder = MPHFbuilder(cfg)           # MPHFbuilder(MPHFconfig)
+    res = builder.build(keys)            # pilots[B * partitions], partition offsets[partitions + 1]
+
+Keys are numpy arrays (uint64 keys, or (n, 2) uint64 / (n, 4) uint32 records), lists
+of bytes (strings), or CUDA tensors (device-resident keys).  The library must be
+built (``python phobic-gpu_b200/build.py``); there is no CPU fallback: every call
+goes through the CUDA kernels or raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libphobic_b200.so"
+FULCRUMS = 2048
+
+OK, ERR_INVALID, ERR_OOM, ERR_BUCKET_OVERFLOW, ERR_PARTITION_OVERFLOW = 0, 1, 2, 3, 4
+ERR_SEARCH_LIMIT, ERR_TIMEOUT, ERR_CUDA, ERR_DUPLICATE_KEY, ERR_BUDGET = 5, 6, 7, 8, 9
+ERR_BUSY, ERR_NO_DEVICE, ERR_NOT_FOUND = 10, 11, 12
+KEYS_U64, KEYS_BYTES16, KEYS_PREHASHED, KEYS_STRINGS = 0, 1, 2, 3
+BUCKETER_OPT, BUCKETER_UNIFORM, BUCKETER_SKEW = 0, 1, 2
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("partition_size", C.c_uint32),
+        ("buckets", C.c_uint32),
+        ("max_partition_size", C.c_uint32),
+        ("max_pilot_counter", C.c_uint32),
+        ("fulcrums", C.c_uint32 * FULCRUMS),
+    ]
+
+
+class Keys(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("on_device", C.c_int32),
+        ("n", C.c_uint64),
+        ("data", C.c_void_p),
+        ("offsets", C.c_void_p),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [("on_device", C.c_int32), ("pilots", C.c_void_p), ("partition_offsets", C.c_void_p)]
+
+
+class Timings(C.Structure):
+    _fields_ = [
+        ("input_transfer", C.c_float),
+        ("bucket_sizes", C.c_float),
+        ("partition_offsets", C.c_float),
+        ("key_redistribution", C.c_float),
+        ("search", C.c_float),
+        ("result_transfer", C.c_float),
+        ("total", C.c_float),
+        ("kernels", C.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int32),
+        ("streams", C.c_uint32),
+        ("queue_capacity", C.c_uint32),
+        ("budget_bytes", C.c_uint64),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("failed", C.c_uint64),
+        ("keys", C.c_uint64),
+        ("p50_ms", C.c_double),
+        ("p99_ms", C.c_double),
+        ("max_ms", C.c_double),
+        ("busy_ms", C.c_double),
+        ("peak_bytes", C.c_uint64),
+    ]
+
+
+class PhobicError(RuntimeError):
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        name = _lib().phobic_status_string(status).decode() if _LIB else str(status)
+        super().__init__(f"{name}{': ' + detail if detail else ''} (status {status})")
+
+
+_LIB: C.CDLL | None = None
+P = C.c_void_p
+PP = C.POINTER(C.c_void_p)
+U32, U64, I32 = C.c_uint32, C.c_uint64, C.c_int
+
+
+def _lib() -> C.CDLL:
+    """Load the in-tree library (raises if it was not built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run python phobic-gpu_b200/build.py")
+    lib = C.CDLL(str(LIB_PATH))
+    sig = {
+        "phobic_status_string": (C.c_char_p, [I32]),
+        "phobic_partitions": (U32, [U64, U32]),
+        "phobic_config": (I32, [C.c_double, U32, I32, I32, C.POINTER(Params)]),
+        "phobic_ctx_create": (I32, [I32, PP]),
+        "phobic_ctx_destroy": (I32, [P]),
+        "phobic_last_error": (C.c_char_p, [P]),
+        "phobic_ctx_device_bytes": (U64, [P]),
+        "phobic_build_bytes_needed": (U64, [C.POINTER(Keys), C.POINTER(Params)]),
+        "phobic_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(Timings)]),
+        "phobic_build_u64": (I32, [P, P, U64, C.POINTER(Params), P, P, C.POINTER(Timings)]),
+        "phobic_build_strings": (I32, [P, P, P, U64, C.POINTER(Params), P, P, C.POINTER(Timings)]),
+        "phobic_build_batch": (I32, [P, C.POINTER(Keys), U32, C.POINTER(Params), C.POINTER(Result), C.POINTER(I32),
+                                     C.POINTER(Timings)]),
+        "phobic_query": (I32, [P, C.POINTER(Keys), C.POINTER(Params), U32, C.POINTER(Result), P]),
+        "phobic_verify": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
+        "phobic_debug_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P, P]),
+        "phobic_server_create": (I32, [C.POINTER(ServerConfig), PP]),
+        "phobic_server_submit": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
+        "phobic_server_poll": (I32, [P, U64, C.POINTER(I32), C.POINTER(I32)]),
+        "phobic_server_wait": (I32, [P, U64, U32, C.POINTER(I32)]),
+        "phobic_server_drain": (I32, [P, U32]),
+        "phobic_server_stats_get": (I32, [P, C.POINTER(ServerStats)]),
+        "phobic_server_destroy": (I32, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype, fn.argtypes = res, args
+    _LIB = lib
+    return lib
+
+
+def lib() -> C.CDLL:
+    return _lib()
+
+
+def check(status: int, ctx: "Context | None" = None) -> None:
+    if status != OK:
+        detail = _lib().phobic_last_error(ctx.handle).decode() if ctx is not None and ctx.handle else ""
+        raise PhobicError(status, detail)
+
+
+# ------------------------------------------------------------------ configuration
+
+class MPHFconfig:
+    """MPHFconfig(λ, P) (mphf_config.h:26-34); bucketer_ctor=True mirrors MPHFconfig(Bucketer*, λ, P)."""
+
+    def __init__(self, average_bucket_size: float = 8.0, partition_size: int = 2048,
+                 bucketer: int = BUCKETER_OPT, bucketer_ctor: bool = False):
+        self.params = Params()
+        check(_lib().phobic_config(float(average_bucket_size), int(partition_size), int(bucketer),
+                                   int(bool(bucketer_ctor)), C.byref(self.params)))
+        self.m_averageBucketSize = float(average_bucket_size)
+        self.partitionSize = int(partition_size)
+        self.bucketCountPerPartition = int(self.params.buckets)
+        self.sortingBins = 256
+
+    def getFulcs(self) -> np.ndarray:
+        return np.ctypeslib.as_array(self.params.fulcrums).copy()
+
+    def partitionMaxSize(self) -> int:
+        return self.partitionSize + self.partitionSize // 2
+
+    def partitions(self, n: int) -> int:
+        return int(_lib().phobic_partitions(int(n), self.partitionSize))
+
+
+# ------------------------------------------------------------------ keys
+
+@dataclass
+class KeySet:
+    """A key set in the layout the C ABI expects; keeps its buffers alive."""
+    kind: int
+    n: int
+    data: object
+    offsets: object = None
+    on_device: bool = False
+    _keep: list = field(default_factory=list)
+
+    def struct(self) -> Keys:
+        return Keys(self.kind, int(self.on_device), self.n, _ptr(self.data), _ptr(self.offsets))
+
+
+def _ptr(x) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data if x.size else None
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr() if x.numel() else None
+    if isinstance(x, int):
+        return x
+    raise TypeError(f"unsupported buffer {type(x)}")
+
+
+def keyset(keys, kind: int | None = None) -> KeySet:
+    """Wrap keys: uint64 array -> U64; (n,2) uint64 -> BYTES16; (n,4) uint32 -> PREHASHED unless kind given;
+    list of bytes/str -> STRINGS; a (bytes, offsets) tuple -> STRINGS; CUDA tensors stay on the device."""
+    if isinstance(keys, KeySet):
+        return keys
+    if isinstance(keys, tuple) and len(keys) == 2:
+        data, offs = keys
+        on_dev = hasattr(data, "is_cuda") and data.is_cuda
+        if not on_dev:
+            data = np.ascontiguousarray(np.frombuffer(data, np.uint8) if isinstance(data, (bytes, bytearray)) else data,
+                                        dtype=np.uint8)
+            offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        return KeySet(KEYS_STRINGS, int(len(offs) - 1), data, offs, on_dev)
+    if isinstance(keys, list):
+        enc = [k.encode() if isinstance(k, str) else bytes(k) for k in keys]
+        offs = np.zeros(len(enc) + 1, np.uint64)
+        np.cumsum([len(e) for e in enc], out=offs[1:])
+        data = np.frombuffer(b"".join(enc), np.uint8) if enc else np.zeros(0, np.uint8)
+        return KeySet(KEYS_STRINGS, len(enc), np.ascontiguousarray(data), offs)
+    if hasattr(keys, "is_cuda") and keys.is_cuda:
+        if keys.dim() == 1:
+            return KeySet(KEYS_U64 if kind is None else kind, int(keys.shape[0]), keys.contiguous(), None, True)
+        return KeySet(KEYS_BYTES16 if kind is None else kind, int(keys.shape[0]), keys.contiguous(), None, True)
+    a = np.ascontiguousarray(keys)
+    if a.ndim == 1:
+        return KeySet(KEYS_U64 if kind is None else kind, a.shape[0], a.astype(np.uint64, copy=False))
+    if a.ndim == 2 and a.dtype == np.uint64 and a.shape[1] == 2:
+        return KeySet(KEYS_BYTES16 if kind is None else kind, a.shape[0], a)
+    if a.ndim == 2 and a.dtype == np.uint32 and a.shape[1] == 4:
+        return KeySet(KEYS_PREHASHED if kind is None else kind, a.shape[0], a)
+    raise TypeError("keys must be uint64[n], uint64[n,2], uint32[n,4], list of bytes, or (bytes, offsets)")
+
+
+# ------------------------------------------------------------------ context
+
+@dataclass
+class BuildResult:
+    pilots: object             # [buckets * partitions] (bucket-major)
+    partition_offsets: object  # [partitions + 1]
+    partitions: int
+    buckets: int
+    timings: dict | None = None
+
+
+class Context:
+    """A phobic_ctx on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        check(_lib().phobic_ctx_create(int(device), C.byref(h)))
+        self.handle = h.value
+        self.device = device
+
+    def close(self) -> None:
+        if self.handle:
+            _lib().phobic_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_error(self) -> str:
+        return _lib().phobic_last_error(self.handle).decode()
+
+    def device_bytes(self) -> int:
+        return int(_lib().phobic_ctx_device_bytes(self.handle))
+
+    def _result(self, cfg: MPHFconfig, n: int, out=None):
+        parts = cfg.partitions(n)
+        if out is not None:
+            pil, off = out
+            return Result(int(_is_cuda(pil)), _ptr(pil), _ptr(off)), pil, off, parts
+        pil = np.zeros(cfg.bucketCountPerPartition * parts, np.uint32)
+        off = np.zeros(parts + 1, np.uint32)
+        return Result(0, _ptr(pil), _ptr(off)), pil, off, parts
+
+    def build(self, keys, cfg: MPHFconfig, out=None, kind: int | None = None) -> BuildResult:
+        ks = keyset(keys, kind)
+        res, pil, off, parts = self._result(cfg, ks.n, out)
+        t = Timings()
+        k = ks.struct()
+        check(_lib().phobic_build(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(t)), self)
+        return BuildResult(pil, off, parts, cfg.bucketCountPerPartition, t.as_dict())
+
+    def debug_build(self, keys, cfg: MPHFconfig, kind: int | None = None):
+        ks = keyset(keys, kind)
+        res, pil, off, parts = self._result(cfg, ks.n)
+        keys4 = np.zeros((max(ks.n, 1), 4), np.uint32)
+        sizes = np.zeros(max(parts * cfg.bucketCountPerPartition, 1), np.uint32)
+        k = ks.struct()
+        check(_lib().phobic_debug_build(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res),
+                                        keys4.ctypes.data, sizes.ctypes.data), self)
+        return (BuildResult(pil, off, parts, cfg.bucketCountPerPartition), keys4[: ks.n],
+                sizes[: parts * cfg.bucketCountPerPartition].reshape(parts, cfg.bucketCountPerPartition))
+
+    def query(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None) -> np.ndarray:
+        ks = keyset(keys, kind)
+        pos = np.zeros(max(ks.n, 1), np.uint32)
+        res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
+        k = ks.struct()
+        check(_lib().phobic_query(self.handle, C.byref(k), C.byref(cfg.params), built.partitions, C.byref(res),
+                                  pos.ctypes.data), self)
+        return pos[: ks.n]
+
+    def verify(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None) -> int:
+        """Number of keys whose slot is out of range or taken twice (0 = bijection)."""
+        ks = keyset(keys, kind)
+        res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
+        bad = C.c_uint64()
+        k = ks.struct()
+        check(_lib().phobic_verify(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(bad)), self)
+        return int(bad.value)
+
+
+def _is_cuda(x) -> bool:
+    return bool(getattr(x, "is_cuda", False))
+
+
+class MPHFbuilder:
+    """MPHFbuilder(MPHFconfig) (mphf_builder.h:36-48): build(keys) -> BuildResult."""
+
+    def __init__(self, config: MPHFconfig | None = None, device: int = 0):
+        self.config = config or MPHFconfig()
+        self.ctx = Context(device)
+
+    def build(self, keys, out=None) -> BuildResult:
+        return self.ctx.build(keys, self.config, out)

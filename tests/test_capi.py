@@ -1,0 +1,102 @@
+"""The C ABI library without a GPU: it loads, exports every symbol that
+include/phobic_b200.h declares, and its host-side arithmetic (MPHFconfig)
+matches the reference's tables.  No compute call is made here."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "phobic_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"PHOBIC_API[^;(]*?\b(phobic_\w+)\s*\(", text, flags=re.S)))
+
+
+def test_header_declares_the_abi():
+    syms = declared_symbols()
+    assert "phobic_build" in syms and "phobic_server_submit" in syms and len(syms) >= 20
+
+
+def test_library_exports_every_declared_symbol(phobic):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(phobic.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = set(re.findall(r" T (phobic_\w+)", out))
+    missing = [s for s in declared_symbols() if s not in exported]
+    assert not missing, missing
+    lib = phobic.lib()
+    for s in declared_symbols():
+        assert getattr(lib, s) is not None
+
+
+def test_library_is_sm100a(phobic):
+    out = subprocess.run(["cuobjdump", "--list-elf", str(phobic.LIB_PATH)], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_config_matches_reference_tables(phobic, golden, golden_fulcrums):
+    for name, meta in golden["fulcrums"].items():
+        cfg = phobic.MPHFconfig(meta["lambda"], meta["P"], meta["bucketer"], bool(meta["bucketer_ctor"]))
+        assert cfg.bucketCountPerPartition == meta["buckets"], name
+        assert (cfg.getFulcs() == golden_fulcrums[name]).all(), name
+        assert cfg.partitionMaxSize() == meta["partition_max_size"]
+        assert cfg.params.max_partition_size == 32 * (meta["partition_max_size"] // 32)
+
+
+def test_config_rejects_bad_arguments(phobic):
+    p = phobic.Params()
+    lib = phobic.lib()
+    assert lib.phobic_config(0.0, 2048, 0, 0, C.byref(p)) == phobic.ERR_INVALID
+    assert lib.phobic_config(5.0, 0, 0, 0, C.byref(p)) == phobic.ERR_INVALID
+    assert lib.phobic_config(5.0, 2048, 7, 0, C.byref(p)) == phobic.ERR_INVALID
+    assert lib.phobic_config(1e-9, 2048, 0, 0, C.byref(p)) == phobic.ERR_INVALID  # buckets > 65535
+
+
+def test_partitions_formula(phobic):
+    lib = phobic.lib()
+    for n, P, want in [(0, 2048, 0), (1, 2048, 1), (2048, 2048, 1), (2049, 2048, 2), (100_000_000, 2500, 40000)]:
+        assert lib.phobic_partitions(n, P) == want
+
+
+def test_status_strings(phobic):
+    lib = phobic.lib()
+    for s in range(13):
+        assert lib.phobic_status_string(s)
+    assert lib.phobic_status_string(999) == b"unknown status"
+
+
+def test_null_context_is_rejected(phobic):
+    lib = phobic.lib()
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    k = phobic.Keys(phobic.KEYS_U64, 0, 0, None, None)
+    r = phobic.Result(0, None, None)
+    assert lib.phobic_build(None, C.byref(k), C.byref(cfg.params), C.byref(r), None) == phobic.ERR_INVALID
+
+
+def test_bytes_needed_formula(phobic):
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    lib = phobic.lib()
+    k = phobic.Keys(phobic.KEYS_U64, 1, 100_000_000, None, None)
+    need = lib.phobic_build_bytes_needed(C.byref(k), C.byref(cfg.params))
+    # device-resident u64 keys: rank 4 + lowers 8 + bucket ids 2 + sorted 8 bytes per key, pilots, offsets
+    assert 22e8 < need < 26e8
+
+
+def test_context_without_device_fails_loudly(phobic):
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(phobic.PhobicError) as e:
+        phobic.Context(0)
+    assert e.value.status == phobic.ERR_NO_DEVICE

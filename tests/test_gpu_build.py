@@ -1,0 +1,198 @@
+"""Parity of the CUDA build path with the oracle, through the C ABI.
+
+Bit-exact comparisons: hashed Keys, bucket sizes, partition offsets and pilots
+equal the oracle's on the same keys and parameters; every build is a bijection
+under the GPU query and under the oracle's query."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import keygen
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def oracle_build(keys4, cfg, **kw):
+    return O.build(keys4, cfg.partitionSize, cfg.bucketCountPerPartition, cfg.getFulcs(), **kw)
+
+
+def check_against_oracle(phobic, ctx, keys, kind, lam, P, debug=True):
+    cfg = phobic.MPHFconfig(lam, P)
+    okind = {phobic.KEYS_U64: "u64", phobic.KEYS_BYTES16: "pairs", phobic.KEYS_STRINGS: "strings"}.get(kind)
+    if kind == phobic.KEYS_PREHASHED:
+        keys4 = np.ascontiguousarray(keys, np.uint32)
+    else:
+        keys4 = O.hash_keys(keys, okind)
+    want = oracle_build(keys4, cfg, intermediates=True)
+    assert want["status"] == 0
+    if debug:
+        got, gkeys4, gsizes = ctx.debug_build(keys, cfg, kind=kind)
+        assert (gkeys4 == keys4).all()
+        assert (gsizes == want["bucket_sizes"]).all()
+    else:
+        got = ctx.build(keys, cfg, kind=kind)
+    assert (got.partition_offsets == want["offsets"]).all()
+    assert (got.pilots == want["pilots"]).all()
+    pos = ctx.query(keys, cfg, got, kind=kind)
+    assert (pos == O.query(keys4, want["partitions"], cfg.bucketCountPerPartition, cfg.getFulcs(), want["pilots"],
+                           want["offsets"])).all()
+    assert O.is_bijection(pos)
+    assert ctx.verify(keys, cfg, got, kind=kind) == 0
+    return got
+
+
+@pytest.mark.parametrize("n", [0, 1, 2, 31, 2047, 2049, 10000, 100_000])
+def test_u64_small_sizes(phobic, ctx, small_builds, n):
+    keys = keygen.splitmix64(1, n)
+    got = check_against_oracle(phobic, ctx, keys, phobic.KEYS_U64, 5.0, 2048)
+    if f"n{n}_pilots" in small_builds:
+        assert (got.pilots == small_builds[f"n{n}_pilots"]).all()
+
+
+def test_c1_u64_matches_golden(phobic, ctx, golden):
+    rec = golden["builds"]["C1_u64_seed1_n1e6_l5_P2048"]
+    keys = keygen.splitmix64(1, 1_000_000)
+    got = check_against_oracle(phobic, ctx, keys, phobic.KEYS_U64, 5.0, 2048)
+    assert sha(got.pilots) == rec["pilots_sha256"]
+    assert sha(got.partition_offsets) == rec["offsets_sha256"]
+
+
+def test_c2_sample_matches_golden(phobic, ctx, golden):
+    rec = golden["builds"]["C2_sample_u64_seed2_n2e6_l7_P2500"]
+    keys = keygen.splitmix64(2, 2_000_000)
+    got = check_against_oracle(phobic, ctx, keys, phobic.KEYS_U64, 7.0, 2500)
+    assert sha(got.pilots) == rec["pilots_sha256"]
+
+
+def test_c3_strings_match_golden(phobic, ctx, golden):
+    rec = golden["builds"]["C3_sample_strings_seed3_n2e4_l6_P2048"]
+    d, o = keygen.strings(3, 20000)
+    got = check_against_oracle(phobic, ctx, (d, o), phobic.KEYS_STRINGS, 6.0, 2048)
+    assert sha(got.pilots) == rec["pilots_sha256"]
+
+
+def test_strings_every_length_0_to_300(phobic, ctx):
+    rng = np.random.default_rng(8)
+    lens = np.concatenate([np.arange(0, 301), rng.integers(0, 300, 3000)])
+    offs = np.zeros(len(lens) + 1, np.uint64)
+    np.cumsum(lens, out=offs[1:])
+    data = rng.integers(0, 256, int(offs[-1]), dtype=np.uint8)
+    # make every string distinct: write its index into the first bytes when long enough
+    for i, L in enumerate(lens):
+        if L >= 4:
+            data[int(offs[i]):int(offs[i]) + 4] = np.frombuffer(np.uint32(i).tobytes(), np.uint8)
+    keys4 = O.hash_keys((data, offs), "strings")
+    uniq = np.unique(keys4, axis=0)
+    keep = len(uniq) == len(keys4)
+    if not keep:
+        pytest.skip("random short strings collided")
+    check_against_oracle(phobic, ctx, (data, offs), phobic.KEYS_STRINGS, 5.0, 512)
+
+
+def test_pairs_and_prehashed(phobic, ctx):
+    pairs = keygen.splitmix64(11, 2 * 50_000).reshape(50_000, 2)
+    check_against_oracle(phobic, ctx, pairs, phobic.KEYS_BYTES16, 6.0, 2048)
+    k4 = keygen.splitmix64(12, 2 * 50_000).view(np.uint32).reshape(50_000, 4)
+    check_against_oracle(phobic, ctx, k4, phobic.KEYS_PREHASHED, 6.0, 2048)
+
+
+@pytest.mark.parametrize("lam,P,bucketer,ctor", [(4.5, 2500, 0, 0), (7.5, 2048, 0, 0), (3.0, 1024, 1, 1),
+                                                 (6.0, 4096, 2, 1), (2.0, 256, 0, 0), (8.0, 8192, 0, 0)])
+def test_configs_and_bucketers(phobic, ctx, lam, P, bucketer, ctor):
+    keys = keygen.splitmix64(21, 60_000)
+    cfg = phobic.MPHFconfig(lam, P, bucketer, bool(ctor))
+    keys4 = O.hash_keys(keys, "u64")
+    want = oracle_build(keys4, cfg)
+    assert want["status"] == 0
+    got = ctx.build(keys, cfg)
+    assert (got.pilots == want["pilots"]).all() and (got.partition_offsets == want["offsets"]).all()
+
+
+def test_device_resident_keys_and_result(phobic, ctx):
+    torch = pytest.importorskip("torch")
+    keys = keygen.splitmix64(2, 300_000)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    parts = cfg.partitions(len(keys))
+    dp = torch.zeros(parts * cfg.bucketCountPerPartition, dtype=torch.int32, device="cuda")
+    do = torch.zeros(parts + 1, dtype=torch.int32, device="cuda")
+    got = ctx.build(dk, cfg, out=(dp, do))
+    want = oracle_build(O.hash_keys(keys, "u64"), cfg)
+    assert (dp.cpu().numpy().view(np.uint32) == want["pilots"]).all()
+    assert (do.cpu().numpy().view(np.uint32) == want["offsets"]).all()
+    assert ctx.verify(dk, cfg, got) == 0
+
+
+def test_bijection_at_ten_million(phobic, ctx):
+    keys = keygen.splitmix64(5, 10_000_000)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    got = ctx.build(keys, cfg)
+    assert ctx.verify(keys, cfg, got) == 0
+    # partition offsets are size-independent facts: last = n, increments = partition sizes
+    assert got.partition_offsets[-1] == len(keys) and (np.diff(got.partition_offsets.astype(np.int64)) >= 0).all()
+
+
+def test_repeated_builds_are_identical(phobic, ctx):
+    keys = keygen.splitmix64(6, 500_000)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    a = ctx.build(keys, cfg)
+    b = ctx.build(keys, cfg)
+    assert (a.pilots == b.pilots).all()
+
+
+# ------------------------------------------------------------------ error paths (host-made inputs)
+
+def test_partition_overflow_is_reported(phobic, ctx):
+    k4 = O.hash_keys(keygen.splitmix64(1, 4000), "u64")
+    k4[:, 0] = 7
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    want = oracle_build(k4, cfg)
+    with pytest.raises(phobic.PhobicError) as e:
+        ctx.build(k4, cfg, kind=phobic.KEYS_PREHASHED)
+    assert e.value.status == want["status"] == phobic.ERR_PARTITION_OVERFLOW
+
+
+def test_bucket_overflow_is_reported(phobic, ctx):
+    k4 = O.hash_keys(keygen.splitmix64(1, 3000), "u64")
+    k4[:300, 1] = 5
+    k4[:300, 0] = k4[0, 0]
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    with pytest.raises(phobic.PhobicError) as e:
+        ctx.build(k4, cfg, kind=phobic.KEYS_PREHASHED)
+    assert e.value.status == oracle_build(k4, cfg)["status"] == phobic.ERR_BUCKET_OVERFLOW
+
+
+def test_duplicate_keys_are_reported(phobic, ctx):
+    keys = keygen.splitmix64(1, 3000)
+    keys[1] = keys[0]
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    with pytest.raises(phobic.PhobicError) as e:
+        ctx.build(keys, cfg)
+    assert e.value.status == oracle_build(O.hash_keys(keys, "u64"), cfg)["status"] == phobic.ERR_DUPLICATE_KEY
+
+
+def test_search_limit_is_reported(phobic, ctx):
+    keys = keygen.splitmix64(1, 4000)
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    cfg.params.max_pilot_counter = 1
+    with pytest.raises(phobic.PhobicError) as e:
+        ctx.build(keys, cfg)
+    want = O.build(O.hash_keys(keys, "u64"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs(), max_k=1)
+    assert e.value.status == want["status"] == phobic.ERR_SEARCH_LIMIT
+
+
+def test_context_survives_errors(phobic, ctx):
+    keys = keygen.splitmix64(1, 3000)
+    keys[1] = keys[0]
+    cfg = phobic.MPHFconfig(5.0, 2048)
+    with pytest.raises(phobic.PhobicError):
+        ctx.build(keys, cfg)
+    good = keygen.splitmix64(1, 3000)
+    got = ctx.build(good, cfg)
+    assert ctx.verify(good, cfg, got) == 0
