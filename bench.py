@@ -1,0 +1,305 @@
+"""Benchmark of the PHOBIC MPHF construction path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n KEYS]
+
+One step = one complete construction of the serialized pilot layout (the part of
+MPHFbuilder::build that the C ABI replaces: hash, partition, bucket sort, pilot
+search) for the headline workload: 100M unique uint64 keys from splitmix64(seed=2),
+lambda=7.0, alpha=1.0, partition size 2500.  Synthetic data, generated from a seed.
+
+Our arm prints one JSON line with
+  value   Mkeys/s over K steps with keys and results resident in HBM, timed with CUDA
+          events on the library's own launching stream (max over ranks);
+  e2e     the same metric through phobic_build with pinned HOST keys and HOST result
+          arrays: every step copies the keys in and the pilots/offsets out;
+  roofline  the search kernel (K4, the dominant one) against measured HBM bandwidth;
+  cpu_baseline  the oracle port of the reference's pipeline on this host's cores.
+The reference arm (--impl reference) times that CPU pipeline on the same workload.
+Under torchrun every rank builds its own independent key set (weak scaling, no
+collective on the data path); rank 0 prints.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "phobic-gpu_b200"))
+
+LAMBDA, PSIZE, SEED = 7.0, 2500, 2
+METRIC = "Mkeys/s MPHF build @100M u64 keys; p50/p99 latency, batched vs plain"
+CONFIG_NAME = "plain build, 100M unique u64 keys splitmix64(seed=2), lambda=7.0, alpha=1.0, partition 2500"
+# Algorithmic bytes of the search kernel per key: read its (lower1, lower2) record (8 B)
+# and bucket id (2 B), write 4 B of pilot per bucket (1/lambda buckets per key).
+K4_BYTES_PER_KEY = 8 + 2 + 4 / LAMBDA
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=5)
+
+    def summary(self) -> dict:
+        sm = [float(r[0]) for r in self.rows if len(r) >= 7 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 7 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 7 for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(n_sample: int, min_seconds: float = 10.0, max_reps: int = 6) -> dict:
+    """Oracle port of the reference pipeline (host hash + stages + search), all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import orc  # the oracle: CPU restatement of the reference's construction
+
+    import keygen
+
+    keys = keygen.splitmix64(SEED, n_sample)
+    B, f = orc.config(LAMBDA, PSIZE)
+    cores = os.cpu_count() or 1
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_reps and (time.perf_counter() - t_start < min_seconds or len(times) < 2):
+        t0 = time.perf_counter()
+        k4 = orc.hash_keys(keys, "u64", threads=cores)
+        r = orc.build(k4, PSIZE, B, f, threads=cores)
+        times.append(time.perf_counter() - t0)
+        assert r["status"] == 0
+    best = min(times)
+    return {"value": n_sample / best / 1e6, "unit": "Mkeys/s", "cores": cores, "kind": "port",
+            "sample": f"first {n_sample} keys of the workload (same lambda/P), {len(times)} runs, best taken",
+            "seconds": sum(times)}
+
+
+def run_reference(args) -> None:
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import orc
+
+    import keygen
+
+    n = args.ref_sample
+    keys = keygen.splitmix64(SEED, n)
+    B, f = orc.config(LAMBDA, PSIZE)
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        orc.build(orc.hash_keys(keys, "u64", threads=cores), PSIZE, B, f, threads=cores)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = orc.build(orc.hash_keys(keys, "u64", threads=cores), PSIZE, B, f, threads=cores)
+        times.append(time.perf_counter() - t0)
+        assert r["status"] == 0
+    ms = 1e3 * sum(times) / len(times)
+    value = n / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seed 2)",
+        "config": {"workload": CONFIG_NAME, "n_keys_per_step": n, "lambda": LAMBDA, "partition_size": PSIZE,
+                   "note": "CPU oracle restatement of the reference pipeline (its Vulkan path cannot run here)"},
+        "cpu_baseline": {"value": value, "unit": "Mkeys/s", "cores": cores, "kind": "port",
+                         "sample": f"{n} keys per step of the headline workload"},
+        "e2e": {"value": value, "unit": "Mkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    import keygen
+    import phobic
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+
+    n = args.n
+    cfg = phobic.MPHFconfig(LAMBDA, PSIZE)
+    keys = keygen.splitmix64(SEED + rank, n)  # every rank: its own independent key set
+    ctx = phobic.Context(local)
+    parts = cfg.partitions(n)
+    B = cfg.bucketCountPerPartition
+
+    # ---- device-resident keys and results
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    dp = torch.empty(parts * B, dtype=torch.int32, device="cuda")
+    do = torch.empty(parts + 1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    for _ in range(args.warmup):
+        ctx.build(dk, cfg, out=(dp, do))
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    search_ms = []
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t_start.record(stream)
+        for _ in range(args.steps):
+            r = ctx.build(dk, cfg, out=(dp, do))
+            search_ms.append(r.timings["search"])
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    dev_ms = t_start.elapsed_time(t_end)
+    stage = dict(r.timings)
+    if pg:
+        t = torch.tensor([dev_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    ms_per_step = dev_ms / args.steps
+    value = world * n / (ms_per_step / 1e3) / 1e6
+
+    # ---- correctness of what was timed: on-device bijection check
+    bad = ctx.verify(dk, cfg, phobic.BuildResult(dp, do, parts, B))
+
+    # ---- end to end through the C ABI with pinned host buffers
+    hk = torch.from_numpy(keys.view(np.int64)).pin_memory()
+    hp = torch.empty(parts * B, dtype=torch.int32).pin_memory()
+    ho = torch.empty(parts + 1, dtype=torch.int32).pin_memory()
+    hks = phobic.KeySet(phobic.KEYS_U64, n, hk.data_ptr())
+    for _ in range(max(1, args.warmup)):
+        ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
+    if pg:
+        pg.barrier()
+    e2e_wall, e2e_dev = [], []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r2 = ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
+        e2e_wall.append(time.perf_counter() - t0)
+        e2e_dev.append(r2.timings["total"])
+    e2e_ms = 1e3 * sum(e2e_wall) / len(e2e_wall)
+    if pg:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    same = bool((hp.numpy() == dp.cpu().numpy()).all())
+
+    if rank != 0:
+        ctx.close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    peaks = measured_peaks()
+    k4_ms = statistics.mean(search_ms)
+    achieved = K4_BYTES_PER_KEY * n / (k4_ms / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "k4_traffic.json"
+    if tp.exists():
+        tr = json.loads(tp.read_text())
+        traffic = tr.get("bytes_per_key", 0) * n if tr.get("bytes_per_key") else None
+    base = cpu_baseline(args.cpu_sample) if not args.no_cpu_baseline else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seed 2 + rank)",
+        "config": {"workload": CONFIG_NAME, "n_keys": n, "lambda": LAMBDA, "alpha": 1.0, "partition_size": PSIZE,
+                   "buckets_per_partition": B, "partitions": parts, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (800 MB keys per step)"},
+        "stages_ms": {k: round(v, 4) for k, v in stage.items() if k != "kernels"},
+        "bijection_bad": bad, "host_result_equals_device": same,
+        "gpu_launches": 4 * args.steps,
+        "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mkeys/s", "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 4 * (parts * B + parts + 1), "ms_per_step": e2e_ms,
+                "device_ms_per_step": statistics.mean(e2e_dev)},
+        "roofline": {"kernel": "k_search (K4)", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"], "bytes_per_key": K4_BYTES_PER_KEY,
+                     "launch_ms": k4_ms},
+        "cpu_baseline": base,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=100_000_000)
+    ap.add_argument("--cpu-sample", type=int, default=20_000_000)
+    ap.add_argument("--ref-sample", type=int, default=20_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -124,6 +124,9 @@ PHOBIC_API phobic_status phobic_ctx_destroy(phobic_ctx *ctx);
 PHOBIC_API const char *phobic_last_error(const phobic_ctx *ctx);
 /* Device bytes the context's pools hold now. */
 PHOBIC_API uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t): every kernel of its builds runs on it, so
+ * callers can order their own work and time builds with events on this stream. */
+PHOBIC_API void *phobic_ctx_stream(const phobic_ctx *ctx);
 /* Device bytes one build of n keys needs (keys staging excluded when on_device). */
 PHOBIC_API uint64_t phobic_build_bytes_needed(const phobic_keys *keys, const phobic_params *params);
 

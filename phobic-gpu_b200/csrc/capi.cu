@@ -1,8 +1,9 @@
 // C ABI entry points (include/phobic_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
+#include <vector>
 
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -99,18 +100,90 @@ const char *phobic_last_error(const phobic_ctx *ctx) { return ctx ? ctx->last_er
 
 uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx) { return ctx ? ctx->w.arena.capacity() : 0; }
 
+void *phobic_ctx_stream(const phobic_ctx *ctx) { return ctx ? static_cast<void *>(ctx->w.stream) : nullptr; }
+
 uint64_t phobic_build_bytes_needed(const phobic_keys *keys, const phobic_params *params) {
     if (!keys || !params || !params->partition_size) return 0;
-    return build_arena_bytes(keys, params, nullptr, false);
+    return sets_arena_bytes(keys, 1, params, nullptr, false);
 }
 
 phobic_status phobic_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
                            const phobic_result *result, phobic_timings *timings) {
     if (!ctx) return PHOBIC_ERR_INVALID;
     ctx->last_error.clear();
-    phobic_status st = enqueue_build(ctx->w, keys, params, result, nullptr, &ctx->last_error);
+    if (!keys || !result) {
+        ctx->last_error = "null keys or result";
+        return PHOBIC_ERR_INVALID;
+    }
+    phobic_status st = enqueue_sets(ctx->w, keys, 1, params, result, nullptr, &ctx->last_error);
     if (st != PHOBIC_OK) return st;
-    return finish_build(ctx->w, timings, &ctx->last_error);
+    return finish_sets(ctx->w, nullptr, timings, &ctx->last_error);
+}
+
+// Sets are built in groups of one key kind and placement whose keys sum to
+// less than 2^32; each group is one launch of each kernel.
+phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *sets, uint32_t nsets,
+                                 const phobic_params *params, const phobic_result *results,
+                                 phobic_status *statuses, phobic_timings *timings) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    if (!sets || !results || !nsets) {
+        ctx->last_error = "no key sets";
+        return PHOBIC_ERR_INVALID;
+    }
+    std::vector<uint32_t> idx(nsets);
+    for (uint32_t i = 0; i < nsets; i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) {
+        return sets[a].kind * 2 + sets[a].on_device < sets[b].kind * 2 + sets[b].on_device;
+    });
+    if (timings) std::memset(timings, 0, sizeof(*timings));
+    phobic_status first = PHOBIC_OK;
+    std::vector<phobic_keys> gk;
+    std::vector<phobic_result> gr;
+    std::vector<uint32_t> gi;
+    std::vector<phobic_status> gs;
+    auto flush = [&]() -> phobic_status {
+        if (gk.empty()) return PHOBIC_OK;
+        gs.assign(gk.size(), PHOBIC_OK);
+        phobic_timings t{};
+        std::string err;
+        phobic_status st = enqueue_sets(ctx->w, gk.data(), (uint32_t)gk.size(), params, gr.data(), nullptr, &err);
+        if (st == PHOBIC_OK) st = finish_sets(ctx->w, gs.data(), &t, &err);
+        else gs.assign(gk.size(), st);
+        if (st != PHOBIC_OK && first == PHOBIC_OK) {
+            first = st;
+            ctx->last_error = err;
+        }
+        for (size_t j = 0; j < gk.size(); j++)
+            if (statuses) statuses[gi[j]] = gs[j];
+        if (timings) {
+            timings->input_transfer += t.input_transfer;
+            timings->bucket_sizes += t.bucket_sizes;
+            timings->partition_offsets += t.partition_offsets;
+            timings->key_redistribution += t.key_redistribution;
+            timings->search += t.search;
+            timings->result_transfer += t.result_transfer;
+            timings->total += t.total;
+            timings->kernels += t.kernels;
+        }
+        gk.clear(), gr.clear(), gi.clear();
+        return st;
+    };
+    uint64_t keys_in_group = 0;
+    for (uint32_t j = 0; j < nsets; j++) {
+        const phobic_keys &k = sets[idx[j]];
+        bool same = !gk.empty() && gk[0].kind == k.kind && gk[0].on_device == k.on_device;
+        if (!gk.empty() && (!same || keys_in_group + k.n > 0xFFFFFFFFull)) {
+            flush();
+            keys_in_group = 0;
+        }
+        gk.push_back(k);
+        gr.push_back(results[idx[j]]);
+        gi.push_back(idx[j]);
+        keys_in_group += k.n;
+    }
+    flush();
+    return first;
 }
 
 phobic_status phobic_build_u64(phobic_ctx *ctx, const uint64_t *keys, uint64_t n, const phobic_params *params,
@@ -132,10 +205,11 @@ phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *keys, const
                                  const phobic_result *result, uint32_t *keys4, uint32_t *bucket_sizes) {
     if (!ctx) return PHOBIC_ERR_INVALID;
     ctx->last_error.clear();
+    if (!keys || !result) return PHOBIC_ERR_INVALID;
     DebugOut dbg{keys4, bucket_sizes};
-    phobic_status st = enqueue_build(ctx->w, keys, params, result, &dbg, &ctx->last_error);
+    phobic_status st = enqueue_sets(ctx->w, keys, 1, params, result, &dbg, &ctx->last_error);
     if (st != PHOBIC_OK) return st;
-    return finish_build(ctx->w, nullptr, &ctx->last_error);
+    return finish_sets(ctx->w, nullptr, nullptr, &ctx->last_error);
 }
 
 phobic_status phobic_query(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params, uint32_t partitions,

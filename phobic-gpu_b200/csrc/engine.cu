@@ -2,17 +2,20 @@
 // (include/phobicGpu/mphf_builder.h:225-292).
 //
 //   reference stage (mphf_builder.h)           here
-//   initialHash (host, :201-216)          ->  K1 map_count (device XXH3)
-//   input_transfer (:233-238)             ->  H2D of the raw keys (16 B Key not materialised)
-//   bucket_sizes (:153-159)               ->  K1
+//   initialHash (host, :201-216)          ->  K1 map_count (XXH3 on the device)
+//   input_transfer (:233-238)             ->  H2D of the raw keys (no 16-byte Key array)
+//   bucket_sizes (:153-159)               ->  K1 (partition counts) + K4 (bucket counts)
 //   bucket_sorting (:162-167)             ->  K4 (shared memory, per partition)
 //   partition_offsets (:169-174)          ->  K2 decoupled-lookback scan
-//   apply_partition_offsets (:176-180)    ->  K3 (offset added while scattering)
+//   apply_partition_offsets (:176-180)    ->  K2 cursors + K3
 //   key_redistribution (:182-187)         ->  K3 + K4
 //   search (:189-194)                     ->  K4
 //   result_transfer (:196-261)            ->  D2H of pilots and offsets
+//
+// A build takes a list of key sets; the plain build is the list of one.
 #include "engine.hpp"
 
+#include <algorithm>
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -22,7 +25,7 @@
 
 namespace phobicb200 {
 
-// ------------------------------------------------------------------ arena
+// ------------------------------------------------------------------ memory
 
 cudaError_t DeviceArena::reserve(size_t bytes) {
     if (bytes <= cap_) return cudaSuccess;
@@ -53,6 +56,25 @@ void *DeviceArena::take(size_t bytes) {
     return p;
 }
 
+cudaError_t PinnedBuffer::reserve(size_t bytes) {
+    if (bytes <= cap_) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMallocHost(&p_, bytes);
+    if (e != cudaSuccess) {
+        p_ = nullptr;
+        cudaGetLastError();
+        return e;
+    }
+    cap_ = bytes;
+    return cudaSuccess;
+}
+
+void PinnedBuffer::release() {
+    if (p_) cudaFreeHost(p_);
+    p_ = nullptr;
+    cap_ = 0;
+}
+
 // ------------------------------------------------------------------ helpers
 
 phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
@@ -64,10 +86,10 @@ phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
     return PHOBIC_ERR_CUDA;
 }
 
-#define PHB_TRY(expr, what)                                        \
-    do {                                                           \
-        phobic_status s_ = cuda_status((expr), (what), err);       \
-        if (s_ != PHOBIC_OK) return s_;                            \
+#define PHB_TRY(expr, what)                                  \
+    do {                                                     \
+        phobic_status s_ = cuda_status((expr), (what), err); \
+        if (s_ != PHOBIC_OK) return s_;                      \
     } while (0)
 
 phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) {
@@ -88,7 +110,7 @@ phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) 
 }
 
 uint32_t default_max_partition(uint32_t P) {
-    uint32_t words = (P + P / 2) / 32;  // mphf_config.h:61-64 / 32 bits (search.comp:21)
+    uint32_t words = (P + P / 2) / 32;  // mphf_config.h:61-64, 32 slots per bitmap word (search.comp:21)
     return 32 * (words ? words : 1);
 }
 
@@ -104,7 +126,7 @@ phobic_status Worker::init(int dev, std::string *err) {
     PHB_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev), "device query");
     PHB_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto &e : ev) PHB_TRY(cudaEventCreate(&e), "cudaEventCreate");
-    PHB_TRY(cudaMallocHost(&pinned_err, sizeof(unsigned long long)), "cudaMallocHost");
+    PHB_TRY(pinned.reserve(1 << 16), "cudaMallocHost");
     if (const char *t = std::getenv("PHOBIC_TIMEOUT_MS")) timeout_ms = std::strtoull(t, nullptr, 10);
     return PHOBIC_OK;
 }
@@ -115,13 +137,13 @@ void Worker::destroy() {
         if (ev[7] && cudaEventRecord(ev[7], stream) == cudaSuccess) wait_event(ev[7], timeout_ms, nullptr);
     }
     arena.release();
+    pinned.release();
     for (auto &e : ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     if (stream) cudaStreamDestroy(stream), stream = nullptr;
-    if (pinned_err) cudaFreeHost(pinned_err), pinned_err = nullptr;
 }
 
-// ------------------------------------------------------------------ sizes
+// ------------------------------------------------------------------ validation and sizes
 
 static uint64_t key_bytes(const phobic_keys *k) {
     switch (k->kind) {
@@ -132,171 +154,220 @@ static uint64_t key_bytes(const phobic_keys *k) {
     }
 }
 
-phobic_status check_build_args(const phobic_keys *keys, const phobic_params *params, uint32_t *cap, uint32_t *k_max,
-                               std::string *err) {
+static uint64_t staged_bytes(const phobic_keys *k) {
+    if (k->on_device) return 0;
+    if (k->kind == PHOBIC_KEYS_STRINGS) return align256(k->n ? k->offsets[k->n] : 0) + align256(8 * (k->n + 1));
+    return align256(key_bytes(k));
+}
+
+phobic_status check_keys(const phobic_keys *keys, std::string *err) {
     auto bad = [&](const char *m) {
         if (err) *err = m;
         return PHOBIC_ERR_INVALID;
     };
-    if (!keys || !params) return bad("null keys or params");
+    if (!keys) return bad("null keys");
     if (keys->kind < PHOBIC_KEYS_U64 || keys->kind > PHOBIC_KEYS_STRINGS) return bad("unknown key kind");
     if (keys->n > 0xFFFFFFFFull) return bad("more than 2^32-1 keys (the reference's uint32 size, mphf_builder.h:56)");
-    if (keys->n && !keys->data) return bad("null key data");
     if (keys->kind == PHOBIC_KEYS_STRINGS && keys->n && !keys->offsets) return bad("strings need offsets");
+    if (keys->kind != PHOBIC_KEYS_STRINGS && keys->n && !keys->data) return bad("null key data");
+    return PHOBIC_OK;
+}
+
+phobic_status check_params(const phobic_params *params, uint32_t *cap, uint32_t *k_max, std::string *err) {
+    auto bad = [&](const char *m) {
+        if (err) *err = m;
+        return PHOBIC_ERR_INVALID;
+    };
+    if (!params) return bad("null params");
     if (params->partition_size == 0) return bad("partition_size must be > 0");
     if (params->buckets == 0 || params->buckets > 65535) return bad("buckets must be in 1..65535");
     if (params->fulcrums[kFulcrums - 1] != (params->buckets << 16))
         return bad("fulcrum table does not end at buckets << 16 (mphf_config.h:54)");
     *cap = params->max_partition_size ? params->max_partition_size : default_max_partition(params->partition_size);
     *k_max = params->max_pilot_counter ? params->max_pilot_counter : kDefaultMaxPilot;
+    if (*cap > 65535) return bad("max_partition_size must be <= 65535");
     if (search_warps_per_cta(params->buckets, *cap) < 1)
         return bad("buckets/partition capacity exceed the search kernel's shared memory");
     return PHOBIC_OK;
 }
 
-uint64_t build_arena_bytes(const phobic_keys *keys, const phobic_params *params, const phobic_result *result,
-                           bool debug) {
-    uint64_t n = keys->n;
-    uint64_t m = (n + params->partition_size - 1) / params->partition_size;
-    uint64_t B = params->buckets;
-    uint64_t t = 0;
-    if (!keys->on_device) {
-        if (keys->kind == PHOBIC_KEYS_STRINGS) t += align256(n ? keys->offsets[n] : 0) + align256(8 * (n + 1));
-        else t += align256(key_bytes(keys));
+uint64_t sets_arena_bytes(const phobic_keys *sets, uint32_t nsets, const phobic_params *params,
+                          const phobic_result *results, bool debug) {
+    const uint64_t P = params->partition_size, B = params->buckets;
+    uint64_t N = 0, M = 0, t = 0;
+    for (uint32_t s = 0; s < nsets; s++) {
+        uint64_t m = (sets[s].n + P - 1) / P;
+        N += sets[s].n;
+        M += m;
+        t += staged_bytes(&sets[s]);
+        if (!results || !results[s].on_device) t += align256(4 * B * m) + align256(4 * (m + 1));
     }
-    t += align256(4 * kFulcrums);
-    t += align256(4 * m) + align256(8 * ((m + kScanTile - 1) / kScanTile) + 8) + align256(8);
-    t += align256(4 * n);                                              // rank
-    if (keys->kind == PHOBIC_KEYS_STRINGS) t += align256(16 * n);      // mapped records
-    t += align256(8 * n) + align256(2 * n) + align256(8 * n);          // lowers, bkt, sorted
-    if (!result || !result->on_device) t += align256(4 * B * m) + align256(4 * (m + 1));
-    if (debug) t += align256(16 * n) + align256(4 * m * B);
+    t += align256(4 * kFulcrums) + align256(sizeof(SetDesc) * nsets) + 2 * align256(8 * (nsets + 1)) +
+         align256(8 * nsets) + align256(64);
+    t += align256(4 * M) + align256(4 * (M + 1)) + align256(8 * ((M + kScanTile - 1) / kScanTile) + 8);
+    if (nsets && sets[0].kind == PHOBIC_KEYS_STRINGS) t += align256(16 * N);
+    t += align256(8 * N) + align256(2 * N) + align256(8 * N);  // lowers, bucket ids, sorted
+    if (debug) t += align256(16 * N) + align256(4 * M * B);
     return t + 4096;
 }
 
 // ------------------------------------------------------------------ build
 
-struct PendingBuild {
-    uint64_t n = 0;
-    uint32_t partitions = 0, buckets = 0;
-    uint32_t *d_pilots = nullptr, *d_off = nullptr;
-    uint32_t *h_pilots = nullptr, *h_off = nullptr;
-    unsigned long long *d_err = nullptr;
-    uint4 *d_dbg_keys = nullptr;
-    uint32_t *d_dbg_sizes = nullptr;
-    DebugOut dbg;
-};
-
-phobic_status enqueue_build(Worker &w, const phobic_keys *keys, const phobic_params *params,
-                            const phobic_result *result, const DebugOut *dbg, std::string *err) {
+phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, const phobic_params *params,
+                           const phobic_result *results, const DebugOut *dbg, std::string *err) {
     uint32_t cap = 0, k_max = 0;
-    phobic_status st = check_build_args(keys, params, &cap, &k_max, err);
+    phobic_status st = check_params(params, &cap, &k_max, err);
     if (st != PHOBIC_OK) return st;
-    if (!result || !result->pilots || !result->partition_offsets) {
-        if (err) *err = "null result arrays";
+    if (!sets || !results || nsets == 0) {
+        if (err) *err = "no key sets";
         return PHOBIC_ERR_INVALID;
     }
-    PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
-    const uint64_t n = keys->n;
+    const int kind = sets[0].kind;
+    const int on_dev = sets[0].on_device;
+    uint64_t N = 0, M = 0;
     const uint32_t P = params->partition_size, B = params->buckets;
-    const uint32_t m = (uint32_t)((n + P - 1) / P);  // mphf_builder.h:90
-    const bool debug = dbg && (dbg->keys4 || dbg->bucket_sizes);
+    for (uint32_t s = 0; s < nsets; s++) {
+        if ((st = check_keys(&sets[s], err)) != PHOBIC_OK) return st;
+        if (sets[s].kind != kind || sets[s].on_device != on_dev) {
+            if (err) *err = "all sets of one build must share key kind and placement";
+            return PHOBIC_ERR_INVALID;
+        }
+        const phobic_result &r = results[s];
+        if (!r.partition_offsets || (!r.pilots && sets[s].n)) {
+            if (err) *err = "null result arrays";
+            return PHOBIC_ERR_INVALID;
+        }
+        N += sets[s].n;
+        M += (sets[s].n + P - 1) / P;
+    }
+    if (N > 0xFFFFFFFFull || M > 0xFFFFFFFFull) {
+        if (err) *err = "a build holds at most 2^32-1 keys in total";
+        return PHOBIC_ERR_INVALID;
+    }
+    const bool debug = dbg && (dbg->keys4 || dbg->bucket_sizes) && nsets == 1;
+    PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
 
-    PendingBuild pb;
-    pb.n = n;
-    pb.partitions = m;
-    pb.buckets = B;
-    if (debug) pb.dbg = *dbg;
+    // Host-side set table (pinned): SetDesc[nsets] | key_base[nsets+1] | part_base[nsets+1] | err[nsets].
+    const size_t tab_desc = align256(sizeof(SetDesc) * nsets), tab_kb = align256(8 * (nsets + 1)),
+                 tab_pb = align256(8 * (nsets + 1)), tab_err = align256(8 * nsets);
+    PHB_TRY(w.pinned.reserve(tab_desc + tab_kb + tab_pb + tab_err), "pinned table");
+    char *tab = static_cast<char *>(w.pinned.data());
+    SetDesc *hdesc = reinterpret_cast<SetDesc *>(tab);
+    uint64_t *hkb = reinterpret_cast<uint64_t *>(tab + tab_desc);
+    uint32_t *hpb = reinterpret_cast<uint32_t *>(tab + tab_desc + tab_kb);
+    w.pending_err = reinterpret_cast<unsigned long long *>(tab + tab_desc + tab_kb + tab_pb);
+    w.pending_sets = nsets;
 
     w.arena.reset();
-    PHB_TRY(w.arena.reserve(build_arena_bytes(keys, params, result, debug)), "device arena");
+    PHB_TRY(w.arena.reserve(sets_arena_bytes(sets, nsets, params, results, debug)), "device arena");
     auto take = [&](size_t b) { return w.arena.take(b); };
-
     cudaStream_t s = w.stream;
     PHB_TRY(cudaEventRecord(w.ev[0], s), "event");
 
-    // Inputs.
-    KeyInput in{keys->data, keys->offsets};
-    if (!keys->on_device && n) {
-        if (keys->kind == PHOBIC_KEYS_STRINGS) {
-            uint64_t nbytes = keys->offsets[n];
-            void *d = take(nbytes);
-            void *o = take(8 * (n + 1));
-            if (nbytes) PHB_TRY(cudaMemcpyAsync(d, keys->data, nbytes, cudaMemcpyHostToDevice, s), "H2D keys");
-            PHB_TRY(cudaMemcpyAsync(o, keys->offsets, 8 * (n + 1), cudaMemcpyHostToDevice, s), "H2D offsets");
-            in = KeyInput{d, static_cast<const uint64_t *>(o)};
-        } else {
-            void *d = take(key_bytes(keys));
-            PHB_TRY(cudaMemcpyAsync(d, keys->data, key_bytes(keys), cudaMemcpyHostToDevice, s), "H2D keys");
-            in = KeyInput{d, nullptr};
+    // Inputs and per-set descriptors.
+    uint64_t kb = 0;
+    uint32_t pb = 0;
+    for (uint32_t i = 0; i < nsets; i++) {
+        const phobic_keys &k = sets[i];
+        SetDesc &d = hdesc[i];
+        std::memset(&d, 0, sizeof(d));
+        d.data = k.data;
+        d.offsets = k.offsets;
+        if (!k.on_device && k.n) {
+            if (kind == PHOBIC_KEYS_STRINGS) {
+                uint64_t nb = k.offsets[k.n];
+                void *dd = take(nb);
+                void *oo = take(8 * (k.n + 1));
+                if (nb) PHB_TRY(cudaMemcpyAsync(dd, k.data, nb, cudaMemcpyHostToDevice, s), "H2D keys");
+                PHB_TRY(cudaMemcpyAsync(oo, k.offsets, 8 * (k.n + 1), cudaMemcpyHostToDevice, s), "H2D offsets");
+                d.data = dd;
+                d.offsets = static_cast<const uint64_t *>(oo);
+            } else {
+                void *dd = take(key_bytes(&k));
+                PHB_TRY(cudaMemcpyAsync(dd, k.data, key_bytes(&k), cudaMemcpyHostToDevice, s), "H2D keys");
+                d.data = dd;
+            }
         }
+        const uint32_t m = (uint32_t)((k.n + P - 1) / P);  // mphf_builder.h:90
+        d.key_base = kb;
+        d.n = (uint32_t)k.n;
+        d.part_base = pb;
+        d.partitions = m;
+        if (results[i].on_device) {
+            d.pilots = results[i].pilots;
+            d.part_off = results[i].partition_offsets;
+        } else {
+            d.pilots = static_cast<uint32_t *>(take(4 * (size_t)B * m));
+            d.part_off = static_cast<uint32_t *>(take(4 * ((size_t)m + 1)));
+        }
+        if (m == 0) PHB_TRY(cudaMemsetAsync(d.part_off, 0, 4, s), "memset");
+        hkb[i] = kb;
+        hpb[i] = pb;
+        kb += k.n;
+        pb += m;
     }
+    hkb[nsets] = kb;
+    hpb[nsets] = pb;
     uint32_t *d_fulcs = static_cast<uint32_t *>(take(4 * kFulcrums));
-    PHB_TRY(cudaMemcpyAsync(d_fulcs, params->fulcrums, 4 * kFulcrums, cudaMemcpyHostToDevice, s), "H2D fulcrums");
-
-    uint32_t *d_count = static_cast<uint32_t *>(take(4 * (size_t)m));
-    uint32_t tiles = (m + kScanTile - 1) / kScanTile;
+    SetDesc *d_desc = static_cast<SetDesc *>(take(sizeof(SetDesc) * nsets));
+    uint64_t *d_kb = static_cast<uint64_t *>(take(8 * (nsets + 1)));
+    uint32_t *d_pb = static_cast<uint32_t *>(take(8 * (nsets + 1)));
+    unsigned long long *d_err = static_cast<unsigned long long *>(take(8 * nsets));
+    uint32_t *d_queue = static_cast<uint32_t *>(take(64));
+    uint32_t *d_count = static_cast<uint32_t *>(take(4 * M));
+    uint32_t *d_G = static_cast<uint32_t *>(take(4 * (M + 1)));
+    const uint32_t tiles = (uint32_t)((M + kScanTile - 1) / kScanTile);
     unsigned long long *d_tiles = static_cast<unsigned long long *>(take(8 * (size_t)tiles + 8));
-    uint32_t *d_tile_ctr = reinterpret_cast<uint32_t *>(d_tiles + tiles);
-    pb.d_err = static_cast<unsigned long long *>(take(8));
-    uint32_t *d_rank = static_cast<uint32_t *>(take(4 * n));
-    uint4 *d_mapped = keys->kind == PHOBIC_KEYS_STRINGS ? static_cast<uint4 *>(take(16 * n)) : nullptr;
-    uint2 *d_lowers = static_cast<uint2 *>(take(8 * n));
-    uint16_t *d_bkt = static_cast<uint16_t *>(take(2 * n));
-    uint2 *d_sorted = static_cast<uint2 *>(take(8 * n));
-    if (result->on_device) {
-        pb.d_pilots = result->pilots;
-        pb.d_off = result->partition_offsets;
-    } else {
-        pb.d_pilots = static_cast<uint32_t *>(take(4 * (size_t)B * m));
-        pb.d_off = static_cast<uint32_t *>(take(4 * ((size_t)m + 1)));
-        pb.h_pilots = result->pilots;
-        pb.h_off = result->partition_offsets;
-    }
-    if (debug) {
-        pb.d_dbg_keys = static_cast<uint4 *>(take(16 * n));
-        pb.d_dbg_sizes = static_cast<uint32_t *>(take(4 * (size_t)m * B));
-    }
-    if (!d_sorted || !pb.d_off || (debug && !pb.d_dbg_sizes)) {
+    uint4 *d_mapped = kind == PHOBIC_KEYS_STRINGS ? static_cast<uint4 *>(take(16 * N)) : nullptr;
+    uint2 *d_lowers = static_cast<uint2 *>(take(8 * N));
+    uint16_t *d_bkt = static_cast<uint16_t *>(take(2 * N));
+    uint2 *d_sorted = static_cast<uint2 *>(take(8 * N));
+    uint4 *d_dbg_keys = debug ? static_cast<uint4 *>(take(16 * N)) : nullptr;
+    uint32_t *d_dbg_sizes = debug ? static_cast<uint32_t *>(take(4 * M * B)) : nullptr;
+    if (!d_sorted || (debug && !d_dbg_sizes)) {
         if (err) *err = "arena sizing error";
         return PHOBIC_ERR_OOM;
     }
-
-    PHB_TRY(cudaMemsetAsync(d_count, 0, 4 * (size_t)m, s), "memset");
+    PHB_TRY(cudaMemcpyAsync(d_fulcs, params->fulcrums, 4 * kFulcrums, cudaMemcpyHostToDevice, s), "H2D fulcrums");
+    PHB_TRY(cudaMemcpyAsync(d_desc, hdesc, sizeof(SetDesc) * nsets, cudaMemcpyHostToDevice, s), "H2D sets");
+    PHB_TRY(cudaMemcpyAsync(d_kb, hkb, 8 * (nsets + 1), cudaMemcpyHostToDevice, s), "H2D sets");
+    PHB_TRY(cudaMemcpyAsync(d_pb, hpb, 4 * (nsets + 1), cudaMemcpyHostToDevice, s), "H2D sets");
+    PHB_TRY(cudaMemsetAsync(d_err, 0xFF, 8 * nsets, s), "memset");
+    PHB_TRY(cudaMemsetAsync(d_queue, 0, 64, s), "memset");
+    PHB_TRY(cudaMemsetAsync(d_count, 0, 4 * M, s), "memset");
     PHB_TRY(cudaMemsetAsync(d_tiles, 0, 8 * (size_t)tiles + 8, s), "memset");
-    PHB_TRY(cudaMemsetAsync(pb.d_err, 0xFF, 8, s), "memset");
-    if (m == 0) PHB_TRY(cudaMemsetAsync(pb.d_off, 0, 4, s), "memset");
+    if (M == 0) PHB_TRY(cudaMemsetAsync(d_G, 0, 4, s), "memset");
     PHB_TRY(cudaEventRecord(w.ev[1], s), "event");
 
-    const int grid_cap = w.sm_count * 8;
-    const int grid = (int)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)grid_cap);
-    if (n) {
-        MapArgs ma{m, B, d_fulcs, d_count, d_rank, d_mapped, debug ? pb.d_dbg_keys : nullptr, pb.d_err};
-        PHB_TRY(launch_map_count(keys->kind, in, n, ma, grid, s), "K1 map_count");
-    }
+    const int grid = (int)std::min<uint64_t>((N + kMapThreads - 1) / kMapThreads, (uint64_t)w.sm_count * 8);
+    MapArgs ma{d_desc, d_kb, nsets, B, N, d_fulcs, d_count, d_mapped, d_dbg_keys, d_lowers, d_bkt, d_err};
+    PHB_TRY(launch_map_count(kind, ma, grid, s), "K1 map_count");
     PHB_TRY(cudaEventRecord(w.ev[2], s), "event");
-    ScanArgs sa{d_count, pb.d_off, m, cap, d_tiles, d_tile_ctr, pb.d_err};
+    ScanArgs sa{d_count, d_G, d_count, (uint32_t)M, cap, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles),
+                d_pb, nsets, d_err};
     PHB_TRY(launch_scan(sa, s), "K2 scan");
     PHB_TRY(cudaEventRecord(w.ev[3], s), "event");
-    if (n) {
-        ScatterArgs xa{m, d_fulcs, pb.d_off, d_rank, d_mapped, d_lowers, d_bkt};
-        PHB_TRY(launch_scatter(keys->kind, in, n, xa, grid, s), "K3 scatter");
-    }
+    PHB_TRY(launch_scatter(kind, ma, grid, s), "K3 scatter");
     PHB_TRY(cudaEventRecord(w.ev[4], s), "event");
-    SearchArgs qa{pb.d_off, d_lowers, d_bkt, d_sorted, pb.d_pilots, debug ? pb.d_dbg_sizes : nullptr,
-                  m, B, cap, k_max, pb.d_err};
-    PHB_TRY(launch_search(qa, s), "K4 search");
+    SearchArgs qa{d_desc, d_pb, nsets, (uint32_t)M, d_G, d_lowers, d_bkt, d_sorted, d_dbg_sizes, B, cap, k_max,
+                  d_queue, d_err};
+    PHB_TRY(launch_search(qa, w.sm_count, s), "K4 search");
     PHB_TRY(cudaEventRecord(w.ev[5], s), "event");
 
-    PHB_TRY(cudaMemcpyAsync(w.pinned_err, pb.d_err, 8, cudaMemcpyDeviceToHost, s), "D2H status");
-    if (!result->on_device) {
-        if (m) PHB_TRY(cudaMemcpyAsync(pb.h_pilots, pb.d_pilots, 4 * (size_t)B * m, cudaMemcpyDeviceToHost, s), "D2H pilots");
-        PHB_TRY(cudaMemcpyAsync(pb.h_off, pb.d_off, 4 * ((size_t)m + 1), cudaMemcpyDeviceToHost, s), "D2H offsets");
+    PHB_TRY(cudaMemcpyAsync(w.pending_err, d_err, 8 * nsets, cudaMemcpyDeviceToHost, s), "D2H status");
+    for (uint32_t i = 0; i < nsets; i++) {
+        if (results[i].on_device) continue;
+        const SetDesc &d = hdesc[i];
+        if (d.partitions)
+            PHB_TRY(cudaMemcpyAsync(results[i].pilots, d.pilots, 4 * (size_t)B * d.partitions, cudaMemcpyDeviceToHost,
+                                    s), "D2H pilots");
+        PHB_TRY(cudaMemcpyAsync(results[i].partition_offsets, d.part_off, 4 * ((size_t)d.partitions + 1),
+                                cudaMemcpyDeviceToHost, s), "D2H offsets");
     }
     if (debug) {
-        if (dbg->keys4 && n) PHB_TRY(cudaMemcpyAsync(dbg->keys4, pb.d_dbg_keys, 16 * n, cudaMemcpyDeviceToHost, s), "D2H keys");
-        if (dbg->bucket_sizes && m)
-            PHB_TRY(cudaMemcpyAsync(dbg->bucket_sizes, pb.d_dbg_sizes, 4 * (size_t)m * B, cudaMemcpyDeviceToHost, s), "D2H sizes");
+        if (dbg->keys4 && N) PHB_TRY(cudaMemcpyAsync(dbg->keys4, d_dbg_keys, 16 * N, cudaMemcpyDeviceToHost, s), "D2H keys");
+        if (dbg->bucket_sizes && M)
+            PHB_TRY(cudaMemcpyAsync(dbg->bucket_sizes, d_dbg_sizes, 4 * M * B, cudaMemcpyDeviceToHost, s), "D2H sizes");
     }
     PHB_TRY(cudaEventRecord(w.ev[6], s), "event");
     return PHOBIC_OK;
@@ -311,7 +382,19 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-phobic_status finish_build(Worker &w, phobic_timings *t, std::string *err) {
+static const char *error_text(uint32_t code) {
+    switch (code) {
+    case PHOBIC_ERR_INVALID: return "a bucket id is >= buckets (fulcrum table)";
+    case PHOBIC_ERR_BUCKET_OVERFLOW: return "a bucket holds more than 256 keys";
+    case PHOBIC_ERR_PARTITION_OVERFLOW: return "a partition exceeds max_partition_size";
+    case PHOBIC_ERR_SEARCH_LIMIT: return "pilot counter reached its limit";
+    case PHOBIC_ERR_TIMEOUT: return "bounded device wait expired";
+    case PHOBIC_ERR_DUPLICATE_KEY: return "two keys of one bucket hash identically (duplicate keys)";
+    default: return "error";
+    }
+}
+
+phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t, std::string *err) {
     phobic_status st = wait_event(w.ev[6], w.timeout_ms, err);
     if (st != PHOBIC_OK) return st;
     if (t) {
@@ -324,15 +407,19 @@ phobic_status finish_build(Worker &w, phobic_timings *t, std::string *err) {
         t->total = elapsed(w.ev[0], w.ev[6]);
         t->kernels = 4;
     }
-    unsigned long long e = *w.pinned_err;
-    if (e == kNoError) return PHOBIC_OK;
-    uint32_t code = (uint32_t)e, part = (uint32_t)(e >> 32);
-    static const char *what[] = {"ok", "a bucket id is >= buckets (fulcrum table)", "oom",
-                                 "a bucket holds more than 256 keys", "a partition exceeds max_partition_size",
-                                 "pilot counter reached its limit", "bounded device wait expired", "cuda",
-                                 "two keys of one bucket hash identically (duplicate keys)"};
-    if (err) *err = std::string(code < 9 ? what[code] : "error") + " (partition " + std::to_string(part) + ")";
-    return (phobic_status)code;
+    phobic_status first = PHOBIC_OK;
+    for (uint32_t i = 0; i < w.pending_sets; i++) {
+        unsigned long long e = w.pending_err[i];
+        phobic_status si = e == kNoError ? PHOBIC_OK : (phobic_status)(uint32_t)e;
+        if (statuses) statuses[i] = si;
+        if (si != PHOBIC_OK && first == PHOBIC_OK) {
+            first = si;
+            if (err)
+                *err = std::string(error_text((uint32_t)e)) + " (set " + std::to_string(i) + ", partition " +
+                       std::to_string((uint32_t)(e >> 32)) + ")";
+        }
+    }
+    return first;
 }
 
 // ------------------------------------------------------------------ query
@@ -343,18 +430,21 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
         if (err) *err = "null argument";
         return PHOBIC_ERR_INVALID;
     }
+    phobic_status st = check_keys(keys, err);
+    if (st != PHOBIC_OK) return st;
     const uint64_t n = keys->n;
     const uint32_t B = params->buckets;
     PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
+    PHB_TRY(w.pinned.reserve(4096), "pinned");
+    unsigned long long *hword = static_cast<unsigned long long *>(w.pinned.data());
     uint64_t bytes = 8192 + align256(4 * kFulcrums) + align256(8) + align256(4 * (size_t)B * partitions) +
-                     align256(4 * ((size_t)partitions + 1)) + align256(4 * n) + align256(4 * ((n + 31) / 32 + 1));
-    if (!keys->on_device)
-        bytes += keys->kind == PHOBIC_KEYS_STRINGS ? align256(n ? keys->offsets[n] : 0) + align256(8 * (n + 1))
-                                                   : align256(key_bytes(keys));
+                     align256(4 * ((size_t)partitions + 1)) + align256(4 * n) + align256(4 * ((n + 31) / 32 + 1)) +
+                     staged_bytes(keys);
     w.arena.reset();
     PHB_TRY(w.arena.reserve(bytes), "device arena");
     cudaStream_t s = w.stream;
-    KeyInput in{keys->data, keys->offsets};
+    const void *data = keys->data;
+    const uint64_t *offs = keys->offsets;
     if (!keys->on_device && n) {
         if (keys->kind == PHOBIC_KEYS_STRINGS) {
             uint64_t nb = keys->offsets[n];
@@ -362,11 +452,11 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
             void *o = w.arena.take(8 * (n + 1));
             if (nb) PHB_TRY(cudaMemcpyAsync(d, keys->data, nb, cudaMemcpyHostToDevice, s), "H2D keys");
             PHB_TRY(cudaMemcpyAsync(o, keys->offsets, 8 * (n + 1), cudaMemcpyHostToDevice, s), "H2D offsets");
-            in = KeyInput{d, static_cast<const uint64_t *>(o)};
+            data = d, offs = static_cast<const uint64_t *>(o);
         } else {
             void *d = w.arena.take(key_bytes(keys));
             PHB_TRY(cudaMemcpyAsync(d, keys->data, key_bytes(keys), cudaMemcpyHostToDevice, s), "H2D keys");
-            in = KeyInput{d, nullptr};
+            data = d;
         }
     }
     uint32_t *d_fulcs = static_cast<uint32_t *>(w.arena.take(4 * kFulcrums));
@@ -377,17 +467,17 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
     if (!built->on_device) {
         uint32_t *a = static_cast<uint32_t *>(w.arena.take(4 * (size_t)B * partitions));
         uint32_t *b = static_cast<uint32_t *>(w.arena.take(4 * ((size_t)partitions + 1)));
-        PHB_TRY(cudaMemcpyAsync(a, built->pilots, 4 * (size_t)B * partitions, cudaMemcpyHostToDevice, s), "H2D pilots");
+        if (partitions)
+            PHB_TRY(cudaMemcpyAsync(a, built->pilots, 4 * (size_t)B * partitions, cudaMemcpyHostToDevice, s),
+                    "H2D pilots");
         PHB_TRY(cudaMemcpyAsync(b, built->partition_offsets, 4 * ((size_t)partitions + 1), cudaMemcpyHostToDevice, s),
                 "H2D offsets");
         d_pil = a, d_off = b;
     }
-    uint32_t n_built = 0;
-    PHB_TRY(cudaMemcpyAsync(w.pinned_err, d_off + partitions, 4, cudaMemcpyDeviceToHost, s), "D2H n");
+    PHB_TRY(cudaMemcpyAsync(hword, d_off + partitions, 4, cudaMemcpyDeviceToHost, s), "D2H n");
     PHB_TRY(cudaEventRecord(w.ev[7], s), "event");
-    phobic_status st0 = wait_event(w.ev[7], w.timeout_ms, err);
-    if (st0 != PHOBIC_OK) return st0;
-    n_built = (uint32_t)*w.pinned_err;
+    if ((st = wait_event(w.ev[7], w.timeout_ms, err)) != PHOBIC_OK) return st;
+    const uint32_t n_built = (uint32_t)(*hword & 0xFFFFFFFFull);
     uint32_t *d_pos = nullptr;
     if (positions) d_pos = keys->on_device ? positions : static_cast<uint32_t *>(w.arena.take(4 * n));
     uint32_t *d_seen = nullptr;
@@ -396,19 +486,14 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
         PHB_TRY(cudaMemsetAsync(d_seen, 0, 4 * ((size_t)n_built / 32 + 1), s), "memset");
     }
     QueryArgs qa{partitions, B, d_fulcs, d_pil, d_off, d_pos, d_seen, d_bad, n_built};
-    int grid = (int)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)w.sm_count * 8);
-    if (n && partitions) PHB_TRY(launch_query(keys->kind, in, n, qa, grid, s), "query");
-    unsigned long long hbad = 0;
-    if (bad) PHB_TRY(cudaMemcpyAsync(w.pinned_err, d_bad, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    const int grid = (int)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)w.sm_count * 8);
+    if (n && partitions) PHB_TRY(launch_query(keys->kind, data, offs, n, qa, grid, s), "query");
+    if (bad) PHB_TRY(cudaMemcpyAsync(hword, d_bad, 8, cudaMemcpyDeviceToHost, s), "D2H");
     if (positions && !keys->on_device && n)
         PHB_TRY(cudaMemcpyAsync(positions, d_pos, 4 * n, cudaMemcpyDeviceToHost, s), "D2H positions");
     PHB_TRY(cudaEventRecord(w.ev[7], s), "event");
-    phobic_status st = wait_event(w.ev[7], w.timeout_ms, err);
-    if (st != PHOBIC_OK) return st;
-    if (bad) {
-        hbad = *w.pinned_err;
-        *bad = hbad + (n != n_built ? (n > n_built ? n - n_built : n_built - n) : 0);
-    }
+    if ((st = wait_event(w.ev[7], w.timeout_ms, err)) != PHOBIC_OK) return st;
+    if (bad) *bad = *hword + (n > n_built ? n - n_built : n_built - n);
     return PHOBIC_OK;
 }
 

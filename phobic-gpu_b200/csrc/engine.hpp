@@ -14,7 +14,7 @@ namespace phobicb200 {
 
 // A grow-only device memory pool carved into 256-byte aligned slices; every
 // slice lives until the next reset().  One arena serves one stream, so reuse
-// across builds is ordered by the stream.
+// across builds is ordered by that stream.
 class DeviceArena {
   public:
     ~DeviceArena() { release(); }
@@ -29,16 +29,31 @@ class DeviceArena {
     size_t cap_ = 0, used_ = 0;
 };
 
+// A grow-only pinned host buffer.
+class PinnedBuffer {
+  public:
+    ~PinnedBuffer() { release(); }
+    cudaError_t reserve(size_t bytes);
+    void *data() const { return p_; }
+    void release();
+
+  private:
+    void *p_ = nullptr;
+    size_t cap_ = 0;
+};
+
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// One CUDA stream with its arena, events and a pinned status word.
+// One CUDA stream with its arena, events and pinned status/table buffers.
 struct Worker {
     int device = 0;
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
     DeviceArena arena;
-    unsigned long long *pinned_err = nullptr;  // host-pinned copy of the device error word
+    PinnedBuffer pinned;  // set table on the way in, per-set error words on the way out
+    uint32_t pending_sets = 0;
+    unsigned long long *pending_err = nullptr;  // host view of the error words of the last build
     uint64_t timeout_ms = 120000;
 
     phobic_status init(int device, std::string *err);
@@ -50,20 +65,22 @@ struct DebugOut {
     uint32_t *bucket_sizes = nullptr;  // host [partitions * buckets]
 };
 
-// Validates arguments; fills the derived capacity and pilot cap.
-phobic_status check_build_args(const phobic_keys *keys, const phobic_params *params, uint32_t *cap,
-                               uint32_t *k_max, std::string *err);
+// Validates parameters; fills the derived capacity and pilot-counter cap.
+phobic_status check_params(const phobic_params *params, uint32_t *cap, uint32_t *k_max, std::string *err);
+phobic_status check_keys(const phobic_keys *keys, std::string *err);
 
-// Device bytes one build needs from a worker's arena.
-uint64_t build_arena_bytes(const phobic_keys *keys, const phobic_params *params, const phobic_result *result,
-                           bool debug);
+// Device bytes one build of these sets needs from a worker's arena.
+uint64_t sets_arena_bytes(const phobic_keys *sets, uint32_t nsets, const phobic_params *params,
+                          const phobic_result *results, bool debug);
 
-// Enqueue one whole build on the worker's stream (no wait).
-phobic_status enqueue_build(Worker &w, const phobic_keys *keys, const phobic_params *params,
-                            const phobic_result *result, const DebugOut *dbg, std::string *err);
+// Enqueue one build of nsets key sets on the worker's stream (no wait).  All sets
+// share one kind and one on_device flag; results[s] receives set s.
+phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, const phobic_params *params,
+                           const phobic_result *results, const DebugOut *dbg, std::string *err);
 
-// Wait for the last enqueued build, decode its status and fill timings.
-phobic_status finish_build(Worker &w, phobic_timings *t, std::string *err);
+// Wait for the last enqueued build; statuses[s] (optional) gets each set's status.
+// Returns the first failing set's status.
+phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t, std::string *err);
 
 // Bounded wait on an event: polls cudaEventQuery until done or timeout.
 phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err);

@@ -1,10 +1,15 @@
 // Kernel argument blocks and launch entry points of the construction pipeline.
 //
-//   K1 map_count  keys -> partition counts + per-key rank        (kernels_map.cu)
-//   K2 scan       partition counts -> partition offsets          (kernels_scan.cu)
+//   K1 map_count  keys -> per-partition key counts                 (kernels_map.cu)
+//   K2 scan       counts -> record offsets + scatter cursors        (kernels_scan.cu)
 //   K3 scatter    keys -> partition-contiguous (lower pair, bucket) records
-//   K4 search     per partition: bucket sort + pilot search       (kernels_search.cu)
-//   Q  query      keys -> slots, bijection check                  (kernels_query.cu)
+//   K4 search     per partition: bucket sort + pilot search         (kernels_search.cu)
+//   Q  query      keys -> slots, bijection check                    (kernels_query.cu)
+//
+// Every kernel works on a list of key sets.  The partitions of all sets form one
+// global partition space (set s owns [part_base[s], part_base[s] + partitions));
+// a plain build is a list of one set, a batched build a list of many, and the
+// same launches serve both.
 #pragma once
 
 #include "common.cuh"
@@ -13,58 +18,79 @@ namespace phobicb200 {
 
 constexpr int kMapThreads = 256;
 constexpr int kScanThreads = 512;
-constexpr int kScanItems = 8;  // elements per thread: one tile = 4096 partitions
+constexpr int kScanItems = 8;  // partitions per thread: one tile = 4096 partitions
 constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kSearchWarps = 8;
+constexpr size_t kSearchSmemLimit = 227 * 1024;
 
-struct KeyInput {
-    const void *data;
-    const uint64_t *offsets;  // strings only
+// One key set of a build.
+struct SetDesc {
+    const void *data;          // u64[n] | 16-byte records[n] | string bytes (device)
+    const uint64_t *offsets;   // strings: [n + 1] into data (device), else null
+    uint64_t key_base;         // first global key index of the set
+    uint32_t n;                // keys
+    uint32_t part_base;        // first global partition
+    uint32_t partitions;       // ceil(n / P)
+    uint32_t pad;
+    uint32_t *pilots;          // [buckets * partitions] output (device)
+    uint32_t *part_off;        // [partitions + 1] output (device)
 };
+
+// Set lookup: the largest s with base[s] <= x, for a table with base[nsets] = total.
+template <typename T>
+__device__ __forceinline__ uint32_t find_set(const T *base, uint32_t nsets, T x) {
+    uint32_t lo = 0, hi = nsets;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(base + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 
 struct MapArgs {
-    uint32_t partitions;
+    const SetDesc *sets;
+    const uint64_t *key_base;  // [nsets + 1] global key index of each set
+    uint32_t nsets;
     uint32_t buckets;
-    const uint32_t *fulcs;  // [2048] device
-    uint32_t *part_count;   // [partitions], zeroed
-    uint32_t *rank;         // [n]
-    uint4 *mapped;          // [n] {p, b, lower1, lower2}, strings only (else null)
-    uint4 *debug_keys;      // [n] hashed Keys, debug builds only (else null)
-    unsigned long long *err;
-};
-
-struct ScatterArgs {
-    uint32_t partitions;
-    const uint32_t *fulcs;
-    const uint32_t *part_off;  // [partitions + 1]
-    const uint32_t *rank;
-    const uint4 *mapped;
-    uint2 *lowers;  // [n]
-    uint16_t *bkt;  // [n]
+    uint64_t total_keys;
+    const uint32_t *fulcs;     // [2048]
+    uint32_t *counts;          // K1: [M] zeroed;   K3: cursors (start = record offset)
+    uint4 *mapped;             // strings: [total] {global partition, bucket, lower1, lower2}
+    uint4 *debug_keys;         // [total] hashed Keys (debug builds) or null
+    uint2 *lowers;             // K3 output [total]
+    uint16_t *bkt;             // K3 output [total]
+    unsigned long long *err;   // [nsets]
 };
 
 struct ScanArgs {
-    const uint32_t *in;            // [m] partition sizes
-    uint32_t *out;                 // [m + 1] exclusive prefix, out[m] = total
+    const uint32_t *in;              // [m] partition sizes
+    uint32_t *out;                   // [m + 1] exclusive prefix, out[m] = total
+    uint32_t *cursor;                // [m] copy of out[0..m) (scatter cursors) or null
     uint32_t m;
-    uint32_t cap;                  // largest allowed partition
-    unsigned long long *tile_state; // [tiles], zeroed: (flag << 32) | value
-    uint32_t *tile_counter;         // zeroed
-    unsigned long long *err;
+    uint32_t cap;                    // largest allowed partition
+    unsigned long long *tile_state;  // [tiles], zeroed: (flag << 32) | value
+    uint32_t *tile_counter;          // zeroed
+    const uint32_t *part_base;       // [nsets + 1] to name the set of an overflowing partition
+    uint32_t nsets;
+    unsigned long long *err;         // [nsets]
 };
 
-// One search job = one partition of one key set.
 struct SearchArgs {
-    const uint32_t *part_off;  // [partitions + 1] (of this set)
-    const uint2 *lowers;       // partition-contiguous records (global key index)
+    const SetDesc *sets;
+    const uint32_t *part_base;  // [nsets + 1]
+    uint32_t nsets;
+    uint32_t M;                 // global partitions
+    const uint32_t *G;          // [M + 1] record offsets
+    const uint2 *lowers;        // partition-contiguous records
     const uint16_t *bkt;
-    uint2 *sorted;             // scratch, same indexing as lowers
-    uint32_t *pilots;          // [buckets * partitions]
-    uint32_t *debug_sizes;     // [partitions * buckets] or null
-    uint32_t partitions;
+    uint2 *sorted;              // scratch, same indexing as lowers
+    uint32_t *debug_sizes;      // [M * buckets] or null
     uint32_t buckets;
     uint32_t cap;
     uint32_t k_max;
-    unsigned long long *err;
+    uint32_t *queue;            // zeroed job counter
+    unsigned long long *err;    // [nsets]
 };
 
 struct QueryArgs {
@@ -79,22 +105,22 @@ struct QueryArgs {
     uint32_t n_built;
 };
 
-// Key of index i for each input kind (hasher.hpp:22-66).
+// Key i of a set, for each input kind (hasher.hpp:22-66).
 template <int KIND>
-__device__ __forceinline__ Key4 load_key(const KeyInput &in, uint64_t i) {
+__device__ __forceinline__ Key4 load_key(const void *data, const uint64_t *offsets, uint64_t i) {
     if constexpr (KIND == PHOBIC_KEYS_U64) {
-        uint64_t v = __ldg(static_cast<const unsigned long long *>(in.data) + i);
+        uint64_t v = __ldg(static_cast<const unsigned long long *>(data) + i);
         return key_from_hash(xxh3::hash_u64(v));
     } else if constexpr (KIND == PHOBIC_KEYS_BYTES16) {
-        const unsigned long long *r = static_cast<const unsigned long long *>(in.data) + 2 * i;
+        const unsigned long long *r = static_cast<const unsigned long long *>(data) + 2 * i;
         return key_from_hash(xxh3::hash_16(__ldg(r), __ldg(r + 1)));
     } else if constexpr (KIND == PHOBIC_KEYS_PREHASHED) {
-        const uint32_t *r = static_cast<const uint32_t *>(in.data) + 4 * i;
+        const uint32_t *r = static_cast<const uint32_t *>(data) + 4 * i;
         return Key4{__ldg(r), __ldg(r + 1), __ldg(r + 2), __ldg(r + 3)};
     } else {
-        uint64_t a = __ldg(reinterpret_cast<const unsigned long long *>(in.offsets) + i);
-        uint64_t b = __ldg(reinterpret_cast<const unsigned long long *>(in.offsets) + i + 1);
-        return key_from_hash(xxh3::hash_bytes(static_cast<const uint8_t *>(in.data) + a, (size_t)(b - a)));
+        uint64_t a = __ldg(reinterpret_cast<const unsigned long long *>(offsets) + i);
+        uint64_t b = __ldg(reinterpret_cast<const unsigned long long *>(offsets) + i + 1);
+        return key_from_hash(xxh3::hash_bytes(static_cast<const uint8_t *>(data) + a, (size_t)(b - a)));
     }
 }
 
@@ -102,13 +128,12 @@ __device__ __forceinline__ Key4 load_key(const KeyInput &in, uint64_t i) {
 size_t search_warp_smem(uint32_t buckets, uint32_t cap);
 // Warps (= partitions in flight) per K4 CTA; 0 when one warp's state does not fit.
 int search_warps_per_cta(uint32_t buckets, uint32_t cap);
-constexpr int kSearchWarps = 8;
-constexpr size_t kSearchSmemLimit = 227 * 1024;
 
-cudaError_t launch_map_count(int kind, const KeyInput &in, uint64_t n, const MapArgs &a, int grid, cudaStream_t st);
-cudaError_t launch_scatter(int kind, const KeyInput &in, uint64_t n, const ScatterArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_map_count(int kind, const MapArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_scatter(int kind, const MapArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_scan(const ScanArgs &a, cudaStream_t st);
-cudaError_t launch_search(const SearchArgs &a, cudaStream_t st);
-cudaError_t launch_query(int kind, const KeyInput &in, uint64_t n, const QueryArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st);
+cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,
+                         cudaStream_t st);
 
 }  // namespace phobicb200

@@ -3,88 +3,100 @@
 // K1 replaces the host initial hash (include/phobicGpu/mphf_builder.h:201-216)
 // and the bucket_sizes stage (shaders/bucket_sizes.comp:21-35): every key is
 // hashed with XXH3-128 on the device, mapped to its partition
-// (key_mapping.glsl:43-45) and bucket (:34-41), and counted per partition; the
-// count returned by the atomic is the key's rank inside its partition.
+// (key_mapping.glsl:43-45) and bucket (:34-41), and counted per partition.
 //
 // K3 replaces apply_partition_offset.comp:9-18 and redistribute_keys.comp:21-53:
-// each key's (lower1, lower2) pair and bucket id land at
-// partition_offset[p] + rank, which makes every partition contiguous.  The
-// bucket order inside a partition is produced later in shared memory by K4.
+// each key's (lower1, lower2) pair and bucket id are appended to its partition
+// through a per-partition cursor that K2 set to the partition's first record.
+// Appending in arrival order keeps each partition's write front inside one or
+// two L2 sectors, so the scattered 8-byte and 2-byte stores merge in L2 before
+// they reach HBM.  The bucket order inside a partition is produced later, in
+// shared memory, by K4.
 #include "kernels.cuh"
 
 namespace phobicb200 {
 
-__device__ __forceinline__ void load_fulcrums(uint32_t *sf, const uint32_t *fulcs) {
-    for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = fulcs[i];
-    __syncthreads();
-}
+namespace {
 
-template <int KIND>
-__global__ void __launch_bounds__(kMapThreads) k_map_count(KeyInput in, uint64_t n, MapArgs a) {
-    __shared__ uint32_t sf[kFulcrums];
-    load_fulcrums(sf, a.fulcs);
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    bool bad = false;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        Key4 k = load_key<KIND>(in, i);
-        uint32_t p = partition_of(k.partitioner, a.partitions);
-        uint32_t b = bucket_of(k.bucketer, sf);
-        bad |= b >= a.buckets;
-        a.rank[i] = atomicAdd(&a.part_count[p], 1u);
-        if (a.mapped) a.mapped[i] = make_uint4(p, b, k.lower1, k.lower2);
-        if (a.debug_keys) a.debug_keys[i] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+struct SetCache {
+    uint32_t s = 0xFFFFFFFFu;
+    uint64_t lo = 0, hi = 0;
+    const void *data = nullptr;
+    const uint64_t *offsets = nullptr;
+    uint32_t part_base = 0, partitions = 0;
+
+    __device__ __forceinline__ void locate(const MapArgs &a, uint64_t g) {
+        if (g >= lo && g < hi) return;
+        s = a.nsets == 1 ? 0u : find_set(a.key_base, a.nsets, g);
+        const SetDesc &d = a.sets[s];
+        lo = d.key_base;
+        hi = d.key_base + d.n;
+        data = d.data;
+        offsets = d.offsets;
+        part_base = d.part_base;
+        partitions = d.partitions;
     }
-    if (bad) report_error(a.err, 0, PHOBIC_ERR_INVALID);
-}
+};
 
-template <int KIND>
-__global__ void __launch_bounds__(kMapThreads) k_scatter(KeyInput in, uint64_t n, ScatterArgs a) {
+}  // namespace
+
+template <int KIND, bool SCATTER>
+__global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     __shared__ uint32_t sf[kFulcrums];
-    if (!a.mapped) load_fulcrums(sf, a.fulcs);
+    constexpr bool kReadMapped = SCATTER && KIND == PHOBIC_KEYS_STRINGS;
+    if (!kReadMapped) {
+        for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
+        __syncthreads();
+    }
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        uint32_t p, b, l1, l2;
-        if (a.mapped) {
-            uint4 r = a.mapped[i];
-            p = r.x, b = r.y, l1 = r.z, l2 = r.w;
+    SetCache c;
+    uint32_t bad_set = 0xFFFFFFFFu;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.total_keys; g += stride) {
+        uint32_t gp, b, l1, l2;
+        if constexpr (kReadMapped) {
+            uint4 r = a.mapped[g];
+            gp = r.x, b = r.y, l1 = r.z, l2 = r.w;
         } else {
-            Key4 k = load_key<KIND>(in, i);
-            p = partition_of(k.partitioner, a.partitions);
+            c.locate(a, g);
+            Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
+            gp = c.part_base + partition_of(k.partitioner, c.partitions);
             b = bucket_of(k.bucketer, sf);
             l1 = k.lower1, l2 = k.lower2;
+            if (!SCATTER) {
+                if (b >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = c.s;
+                if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+            }
         }
-        uint32_t dst = a.part_off[p] + a.rank[i];
-        a.lowers[dst] = make_uint2(l1, l2);
-        a.bkt[dst] = (uint16_t)b;
+        if constexpr (SCATTER) {
+            uint32_t slot = atomicAdd(&a.counts[gp], 1u);
+            a.lowers[slot] = make_uint2(l1, l2);
+            a.bkt[slot] = (uint16_t)b;
+        } else {
+            atomicAdd(&a.counts[gp], 1u);
+            if (KIND == PHOBIC_KEYS_STRINGS) a.mapped[g] = make_uint4(gp, b, l1, l2);
+        }
     }
+    if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
 }
 
-template <int KIND>
-static cudaError_t launch_map_kind(const KeyInput &in, uint64_t n, const MapArgs &m, const ScatterArgs &s, int grid,
-                                   cudaStream_t st, bool scatter) {
-    if (scatter) k_scatter<KIND><<<grid, kMapThreads, 0, st>>>(in, n, s);
-    else k_map_count<KIND><<<grid, kMapThreads, 0, st>>>(in, n, m);
+template <bool SCATTER>
+static cudaError_t launch_map(int kind, const MapArgs &a, int grid, cudaStream_t st) {
+    if (a.total_keys == 0) return cudaSuccess;
+    switch (kind) {
+    case PHOBIC_KEYS_U64: k_map<PHOBIC_KEYS_U64, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
+    case PHOBIC_KEYS_BYTES16: k_map<PHOBIC_KEYS_BYTES16, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
+    case PHOBIC_KEYS_PREHASHED: k_map<PHOBIC_KEYS_PREHASHED, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
+    default: k_map<PHOBIC_KEYS_STRINGS, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
+    }
     return cudaGetLastError();
 }
 
-cudaError_t launch_map_count(int kind, const KeyInput &in, uint64_t n, const MapArgs &a, int grid, cudaStream_t st) {
-    ScatterArgs none{};
-    switch (kind) {
-    case PHOBIC_KEYS_U64: return launch_map_kind<PHOBIC_KEYS_U64>(in, n, a, none, grid, st, false);
-    case PHOBIC_KEYS_BYTES16: return launch_map_kind<PHOBIC_KEYS_BYTES16>(in, n, a, none, grid, st, false);
-    case PHOBIC_KEYS_PREHASHED: return launch_map_kind<PHOBIC_KEYS_PREHASHED>(in, n, a, none, grid, st, false);
-    default: return launch_map_kind<PHOBIC_KEYS_STRINGS>(in, n, a, none, grid, st, false);
-    }
+cudaError_t launch_map_count(int kind, const MapArgs &a, int grid, cudaStream_t st) {
+    return launch_map<false>(kind, a, grid, st);
 }
 
-cudaError_t launch_scatter(int kind, const KeyInput &in, uint64_t n, const ScatterArgs &a, int grid, cudaStream_t st) {
-    MapArgs none{};
-    switch (kind) {
-    case PHOBIC_KEYS_U64: return launch_map_kind<PHOBIC_KEYS_U64>(in, n, none, a, grid, st, true);
-    case PHOBIC_KEYS_BYTES16: return launch_map_kind<PHOBIC_KEYS_BYTES16>(in, n, none, a, grid, st, true);
-    case PHOBIC_KEYS_PREHASHED: return launch_map_kind<PHOBIC_KEYS_PREHASHED>(in, n, none, a, grid, st, true);
-    default: return launch_map_kind<PHOBIC_KEYS_STRINGS>(in, n, none, a, grid, st, true);
-    }
+cudaError_t launch_scatter(int kind, const MapArgs &a, int grid, cudaStream_t st) {
+    return launch_map<true>(kind, a, grid, st);
 }
 
 }  // namespace phobicb200

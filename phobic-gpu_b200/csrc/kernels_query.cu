@@ -12,14 +12,15 @@
 namespace phobicb200 {
 
 template <int KIND>
-__global__ void __launch_bounds__(kMapThreads) k_query(KeyInput in, uint64_t n, QueryArgs a) {
+__global__ void __launch_bounds__(kMapThreads) k_query(const void *data, const uint64_t *offsets, uint64_t n,
+                                                      QueryArgs a) {
     __shared__ uint32_t sf[kFulcrums];
     for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
     __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     unsigned long long bad = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        Key4 k = load_key<KIND>(in, i);
+        Key4 k = load_key<KIND>(data, offsets, i);
         uint32_t p = partition_of(k.partitioner, a.partitions);
         uint64_t b = bucket_of_query(k.bucketer, sf);
         uint32_t pos = 0xFFFFFFFFu;
@@ -45,12 +46,13 @@ __global__ void __launch_bounds__(kMapThreads) k_query(KeyInput in, uint64_t n, 
     if (a.bad && bad) atomicAdd(a.bad, bad);
 }
 
-cudaError_t launch_query(int kind, const KeyInput &in, uint64_t n, const QueryArgs &a, int grid, cudaStream_t st) {
+cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,
+                         cudaStream_t st) {
     switch (kind) {
-    case PHOBIC_KEYS_U64: k_query<PHOBIC_KEYS_U64><<<grid, kMapThreads, 0, st>>>(in, n, a); break;
-    case PHOBIC_KEYS_BYTES16: k_query<PHOBIC_KEYS_BYTES16><<<grid, kMapThreads, 0, st>>>(in, n, a); break;
-    case PHOBIC_KEYS_PREHASHED: k_query<PHOBIC_KEYS_PREHASHED><<<grid, kMapThreads, 0, st>>>(in, n, a); break;
-    default: k_query<PHOBIC_KEYS_STRINGS><<<grid, kMapThreads, 0, st>>>(in, n, a); break;
+    case PHOBIC_KEYS_U64: k_query<PHOBIC_KEYS_U64><<<grid, kMapThreads, 0, st>>>(data, offsets, n, a); break;
+    case PHOBIC_KEYS_BYTES16: k_query<PHOBIC_KEYS_BYTES16><<<grid, kMapThreads, 0, st>>>(data, offsets, n, a); break;
+    case PHOBIC_KEYS_PREHASHED: k_query<PHOBIC_KEYS_PREHASHED><<<grid, kMapThreads, 0, st>>>(data, offsets, n, a); break;
+    default: k_query<PHOBIC_KEYS_STRINGS><<<grid, kMapThreads, 0, st>>>(data, offsets, n, a); break;
     }
     return cudaGetLastError();
 }

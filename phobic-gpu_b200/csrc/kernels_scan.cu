@@ -4,7 +4,8 @@
 // prefix_sum_offset.comp:13-19, driven by PrefixSumStage::addCommands,
 // src/prefix_sum_stage.cpp:42-86) and the host's leading zero
 // (include/phobicGpu/mphf_builder.h:254-257): out[0] = 0, out[p + 1] = out[p] + size[p].
-// It also checks every partition against the search bitmap capacity, which the
+// It also seeds the scatter cursors of K3 (a copy of the exclusive prefix) and
+// checks every partition against the search bitmap capacity, which the
 // reference leaves unchecked (search.comp:21).
 //
 // Each CTA takes the next tile id from a counter, so every tile it waits on was
@@ -46,7 +47,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
         if (v[j] > a.cap && over_at == 0xFFFFFFFFu) over_at = (uint32_t)idx;
         sum += v[j];
     }
-    if (over_at != 0xFFFFFFFFu) report_error(a.err, over_at, PHOBIC_ERR_PARTITION_OVERFLOW);
+    if (over_at != 0xFFFFFFFFu) {
+        uint32_t set = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, over_at);
+        report_error(&a.err[set], over_at - a.part_base[set], PHOBIC_ERR_PARTITION_OVERFLOW);
+    }
 
     uint32_t incl = warp_incl_scan(sum, lane);
     if (lane == 31) s_warp[warp] = incl;
@@ -73,7 +77,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
                 unsigned long long flag = s & ~0xFFFFFFFFull;
                 if (flag == 0) {
                     if (++spins > kSpinLimit) {
-                        report_error(a.err, 0, PHOBIC_ERR_TIMEOUT);
+                        for (uint32_t q = 0; q < a.nsets; q++) report_error(&a.err[q], 0, PHOBIC_ERR_TIMEOUT);
                         break;
                     }
                     continue;
@@ -92,7 +96,10 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
         uint64_t idx = base + j;
-        if (idx < a.m) a.out[idx] = run;
+        if (idx < a.m) {
+            a.out[idx] = run;
+            if (a.cursor) a.cursor[idx] = run;
+        }
         run += v[j];
     }
     // The thread holding the last element also writes the total.

@@ -1,4 +1,5 @@
-// K4: per-partition bucket sort and pilot search, one warp per partition.
+// K4: per-partition bucket sort and pilot search; persistent warps, one
+// partition per warp at a time, taken from a shared work queue.
 //
 // Replaces sort_sum.comp:141-226 (bucket histogram, descending-size order,
 // in-partition offsets), redistribute_keys.comp:21-53 (bucket order inside the
@@ -15,48 +16,75 @@
 //   * pilots are stored bucket-major at pilots[b * partitions + p]
 //     (search.comp:170-174); empty buckets get 0.
 //
-// The offset search tests 32 offsets per lane with one funnel shift per key:
-// the occupancy bitmap keeps a copy of its first 32 bits after bit ps, so the
-// 32-bit window starting at any slot < ps reads circularly.  A warp covers
-// 1024 consecutive offsets per round; the first lane with a free window holds
-// the smallest valid offset.
+// Work queue: every warp takes the next global partition from one counter, so
+// partitions of very different cost (and of different key sets in a batched
+// build) spread over the SMs without CTA-level tail imbalance.
+//
+// Offset search: the occupancy bitmap keeps a copy of its first 32 bits after
+// bit ps, so the 32-bit window that starts at any slot < ps reads circularly
+// with one funnel shift.  Lane L tests offsets [w, w+32), w = w0 + 32 L, by
+// OR-ing the windows of all keys; a warp covers 1024 offsets per round and the
+// first lane with a free window holds the smallest valid offset.
+//
+// Buckets of at most 32 keys (nearly all of them) keep one key per lane in
+// registers, test collisions with __match_any_sync and broadcast slots with
+// shuffles; larger buckets stage keys and slots in shared memory.
 #include "kernels.cuh"
 
 namespace phobicb200 {
 
 namespace {
 
-constexpr int kMaxPerLane = kMaxBucket / 32;  // keys of one bucket held per lane
+constexpr uint32_t kNone = 0xFFFFFFFFu;
 
-__device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (cap + 31) / 32 + 2; }
+__host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (cap + 31) / 32 + 2; }
+__host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B + 1) / 2; }
 
-struct WarpSmem {
-    uint32_t *cnt;    // [B] keys per bucket
-    uint32_t *cur;    // [B] scatter cursor; after the scatter: bucket end
-    uint16_t *order;  // [B] bucket ids in search order
-    uint32_t *occ;    // [OW] occupied slots, bits [ps, ps+32) mirror [0, 32)
-    uint32_t *scr;    // [OW] scratch bitmap for collision checks of large buckets
-    uint32_t *binPos; // [256] bin cursor in `order`      (prep phase)
-    uint32_t *binKey; // [256] bin cursor in key positions (prep phase)
-    uint32_t *hs;     // [256] slots of the current bucket (search phase, aliases binPos)
-};
-
+// Per-warp shared memory, in 32-bit words:
+//   sched [B]        search schedule, in search order: start | size << 16
+//   order [B/2]      bucket id (u16) in search order
+//   occ   [OW]       occupied slots, bits [ps, ps+32) mirror [0, 32)
+//   scr   [OW]       collision scratch of large buckets
+//   union of
+//     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
+//     search phase:  hs [256] slots, kl uint2[256] keys of a large bucket
 __host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
-    return 2 * (size_t)B + (B + 1) / 2 + 2 * (size_t)((cap + 31) / 32 + 2) + 512;
+    size_t prep = 2 * (size_t)half_words(B) + 512, search = 256 + 512;
+    return (size_t)B + half_words(B) + 2 * (size_t)occ_words(cap) + (prep > search ? prep : search);
 }
 
-__device__ __forceinline__ WarpSmem carve(uint32_t *base, uint32_t B, uint32_t cap) {
-    WarpSmem w;
-    uint32_t ow = occ_words(cap);
-    w.cnt = base;
-    w.cur = w.cnt + B;
-    w.order = reinterpret_cast<uint16_t *>(w.cur + B);
-    w.occ = w.cur + B + (B + 1) / 2;
-    w.scr = w.occ + ow;
-    w.binPos = w.scr + ow;
-    w.binKey = w.binPos + 256;
-    w.hs = w.binPos;
-    return w;
+struct WarpSmem {
+    uint32_t *sched;
+    uint16_t *order;
+    uint32_t *occ, *scr;
+    uint32_t *cnt32, *cur32;  // packed u16 pairs
+    uint16_t *cur16;
+    uint32_t *binPos, *binKey;
+    uint32_t *hs;
+    uint2 *kl;
+};
+
+__device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap) {
+    WarpSmem m;
+    m.sched = w;
+    m.order = reinterpret_cast<uint16_t *>(w + B);
+    m.occ = w + B + half_words(B);
+    m.scr = m.occ + occ_words(cap);
+    uint32_t *u = m.scr + occ_words(cap);
+    m.cnt32 = u;
+    m.cur32 = u + half_words(B);
+    m.cur16 = reinterpret_cast<uint16_t *>(m.cur32);
+    m.binPos = u + 2 * half_words(B);
+    m.binKey = m.binPos + 256;
+    m.hs = u;
+    m.kl = reinterpret_cast<uint2 *>(u + 256);
+    return m;
+}
+
+__device__ __forceinline__ uint32_t half_get(const uint32_t *w, uint32_t b) { return (w[b >> 1] >> ((b & 1) << 4)) & 0xFFFFu; }
+__device__ __forceinline__ uint32_t half_add(uint32_t *w, uint32_t b) {
+    uint32_t sh = (b & 1) << 4;
+    return (atomicAdd(&w[b >> 1], 1u << sh) >> sh) & 0xFFFFu;
 }
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
@@ -68,49 +96,171 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
     return v;
 }
 
-}  // namespace
+__device__ __forceinline__ void mark(uint32_t *occ, uint32_t q, uint32_t ps) {
+    atomicOr(&occ[q >> 5], 1u << (q & 31));
+    if (q < 32) {
+        uint32_t m = q + ps;
+        atomicOr(&occ[m >> 5], 1u << (m & 31));
+    }
+}
 
-size_t search_warp_smem(uint32_t buckets, uint32_t cap) { return 4 * warp_words(buckets, cap); }
+// Smallest free offset for slots held one per lane (lanes < s).
+__device__ __forceinline__ uint32_t offset_small(const uint32_t *occ, uint32_t h, uint32_t s, uint32_t ps, int lane) {
+    for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
+        const uint32_t w = w0 + 32 * lane;
+        const bool live = w < ps;
+        const uint32_t wl = live ? w : 0u;
+        uint32_t bad = live ? 0u : kFullMask;
+#pragma unroll 4
+        for (uint32_t i = 0; i < s; i++) {
+            uint32_t x = __shfl_sync(kFullMask, h, i) + wl;
+            if (x >= ps) x -= ps;
+            bad |= __funnelshift_r(occ[x >> 5], occ[(x >> 5) + 1], x & 31);
+        }
+        uint32_t valid = ~bad;
+        if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
+        uint32_t ball = __ballot_sync(kFullMask, valid != 0);
+        if (ball) {
+            int f = __ffs(ball) - 1;
+            return w0 + 32 * f + __ffs(__shfl_sync(kFullMask, valid, f)) - 1;
+        }
+    }
+    return kNone;
+}
 
-__global__ void __launch_bounds__(kSearchWarps * 32) k_search(SearchArgs a) {
-    extern __shared__ uint32_t smem[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t p = blockIdx.x * (blockDim.x >> 5) + warp;
-    if (p >= a.partitions) return;
-    if (fatal_before_search(*reinterpret_cast<volatile unsigned long long *>(a.err))) return;
+// Smallest free offset for slots staged in shared memory (any s <= 256).
+__device__ __forceinline__ uint32_t offset_large(const uint32_t *occ, const uint32_t *hs, uint32_t s, uint32_t ps,
+                                                 int lane) {
+    for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
+        const uint32_t w = w0 + 32 * lane;
+        const bool live = w < ps;
+        const uint32_t wl = live ? w : 0u;
+        uint32_t bad = live ? 0u : kFullMask;
+        for (uint32_t i = 0; i < s; i += 8) {
+            uint32_t e = min(s, i + 8);
+            for (uint32_t t = i; t < e; t++) {
+                uint32_t x = hs[t] + wl;
+                if (x >= ps) x -= ps;
+                bad |= __funnelshift_r(occ[x >> 5], occ[(x >> 5) + 1], x & 31);
+            }
+            if (__all_sync(kFullMask, bad == kFullMask)) break;
+        }
+        uint32_t valid = ~bad;
+        if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
+        uint32_t ball = __ballot_sync(kFullMask, valid != 0);
+        if (ball) {
+            int f = __ffs(ball) - 1;
+            return w0 + 32 * f + __ffs(__shfl_sync(kFullMask, valid, f)) - 1;
+        }
+    }
+    return kNone;
+}
 
+// One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
+__device__ __forceinline__ uint32_t place_small(uint32_t *occ, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
+                                                uint32_t k_lim, int lane, uint32_t *pilot) {
+    const bool mine = lane < (int)s;
+    for (uint32_t k = 0; k < k_lim; k++) {
+        if (k == kDupCheckAt && s > 1) {
+            bool d = false;
+            for (uint32_t t = 0; t + 1 < s; t++) {
+                uint32_t x = __shfl_sync(kFullMask, L.x, t), y = __shfl_sync(kFullMask, L.y, t);
+                d |= mine && lane > (int)t && L.x == x && L.y == y;
+            }
+            if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
+        }
+        const uint32_t h = mine ? fm.mod(pilot_hash(L.x, L.y, k)) : (0x80000000u | lane);
+        if (s > 1) {
+            uint32_t m = __match_any_sync(kFullMask, h);
+            if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
+        }
+        const uint32_t o = offset_small(occ, h, s, ps, lane);
+        if (o == kNone) continue;
+        if (mine) {
+            uint32_t q = h + o;
+            mark(occ, q >= ps ? q - ps : q, ps);
+        }
+        __syncwarp();
+        *pilot = o + ps * k;
+        return PHOBIC_OK;
+    }
+    return PHOBIC_ERR_SEARCH_LIMIT;
+}
+
+// One bucket of more than 32 keys, staged in shared memory (ws.kl, ws.hs).
+__device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 *src, uint32_t s, uint32_t ps,
+                                                FastMod fm, uint32_t k_lim, int lane, uint32_t *pilot) {
+    for (uint32_t i = lane; i < s; i += 32) ws.kl[i] = src[i];
+    __syncwarp();
+    for (uint32_t k = 0; k < k_lim; k++) {
+        if (k == kDupCheckAt) {
+            bool d = false;
+            for (uint32_t t = 0; t + 1 < s; t++) {
+                uint2 kt = ws.kl[t];
+                for (uint32_t i = lane; i < s; i += 32) d |= i > t && ws.kl[i].x == kt.x && ws.kl[i].y == kt.y;
+            }
+            if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
+        }
+        bool d = false;
+        for (uint32_t i = lane; i < s; i += 32) {
+            uint2 key = ws.kl[i];
+            uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
+            ws.hs[i] = h;
+            uint32_t bit = 1u << (h & 31);
+            d |= (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+        }
+        const bool dup = __any_sync(kFullMask, d);
+        for (uint32_t i = lane; i < s; i += 32) ws.scr[ws.hs[i] >> 5] = 0;
+        __syncwarp();
+        if (dup) continue;
+        const uint32_t o = offset_large(ws.occ, ws.hs, s, ps, lane);
+        if (o == kNone) continue;
+        for (uint32_t i = lane; i < s; i += 32) {
+            uint32_t q = ws.hs[i] + o;
+            mark(ws.occ, q >= ps ? q - ps : q, ps);
+        }
+        __syncwarp();
+        *pilot = o + ps * k;
+        return PHOBIC_OK;
+    }
+    return PHOBIC_ERR_SEARCH_LIMIT;
+}
+
+// One partition: bucket histogram, search order, bucket-sorted keys, pilots.
+__device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
+                                                     uint32_t g, uint32_t p, int lane) {
     const uint32_t B = a.buckets;
-    WarpSmem ws = carve(smem + (size_t)warp * warp_words(B, a.cap), B, a.cap);
-    const uint32_t base = a.part_off[p];
-    const uint32_t ps = a.part_off[p + 1] - base;
-    if (ps > a.cap) return;  // reported by the scan
+    const uint32_t base = a.G[g];
+    const uint32_t ps = a.G[g + 1] - base;
+    if (ps > a.cap) return PHOBIC_OK;  // reported by the scan
     const uint32_t ow = occ_words(a.cap);
+    uint32_t *pil = d.pilots + p;
+    const size_t pstride = d.partitions;
 
-    for (uint32_t i = lane; i < B; i += 32) ws.cnt[i] = 0;
+    for (uint32_t i = lane; i < half_words(B); i += 32) ws.cnt32[i] = 0;
     for (uint32_t i = lane; i < ow; i += 32) ws.occ[i] = 0, ws.scr[i] = 0;
     for (uint32_t i = lane; i < 512; i += 32) ws.binPos[i] = 0;
     __syncwarp();
 
-    // Bucket sizes (bucket_sizes.comp:21-35, restricted to this partition).
-    for (uint32_t i = lane; i < ps; i += 32) atomicAdd(&ws.cnt[a.bkt[base + i]], 1u);
+    // Bucket sizes of this partition (bucket_sizes.comp:21-35).
+    const uint16_t *bk = a.bkt + base;
+#pragma unroll 4
+    for (uint32_t i = lane; i < ps; i += 32) half_add(ws.cnt32, bk[i]);
     __syncwarp();
 
     // Size histogram in bins 256 - size (sort_sum.comp:56-58,166-170); empty buckets get pilot 0.
     bool over = false;
     for (uint32_t b = lane; b < B; b += 32) {
-        uint32_t s = ws.cnt[b];
-        if (a.debug_sizes) a.debug_sizes[(size_t)p * B + b] = s;
+        uint32_t s = half_get(ws.cnt32, b);
+        if (a.debug_sizes) a.debug_sizes[(size_t)g * B + b] = s;
         if (s > kMaxBucket) over = true;
         else if (s) atomicAdd(&ws.binPos[kBins - s], 1u);
-        else a.pilots[(size_t)b * a.partitions + p] = 0;
+        else pil[(size_t)b * pstride] = 0;
     }
-    if (__any_sync(kFullMask, over)) {
-        if (lane == 0) report_error(a.err, p, PHOBIC_ERR_BUCKET_OVERFLOW);
-        return;
-    }
+    if (__any_sync(kFullMask, over)) return PHOBIC_ERR_BUCKET_OVERFLOW;
     __syncwarp();
 
-    // Exclusive prefix over bins of bucket counts and of key counts (sort_sum.comp:184-215).
+    // Exclusive prefix over bins of bucket counts and key counts (sort_sum.comp:184-215).
     uint32_t c[8], loc = 0, lock = 0;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
@@ -119,7 +269,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(SearchArgs a) {
         loc += c[j];
         lock += c[j] * (kBins - bin);
     }
-    uint32_t inc = warp_incl_scan(loc, lane), inck = warp_incl_scan(lock, lane);
+    const uint32_t inc = warp_incl_scan(loc, lane), inck = warp_incl_scan(lock, lane);
     const uint32_t nonempty = __shfl_sync(kFullMask, inc, 31);
     uint32_t ex = inc - loc, exk = inck - lock;
     __syncwarp();
@@ -133,16 +283,18 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(SearchArgs a) {
     }
     __syncwarp();
 
-    // Search order: within a bin, higher bucket index first (sort_sum.comp:156).
+    // Search order: within a bin, the higher bucket index first (sort_sum.comp:156).
     for (uint32_t c0 = 0; c0 < B; c0 += 32) {
-        int bi = (int)B - 1 - (int)(c0 + lane);
-        uint32_t s = bi >= 0 ? ws.cnt[bi] : 0u;
-        uint32_t peers = __match_any_sync(kFullMask, s ? s : 0x10000u + lane);
-        uint32_t r = __popc(peers & lanemask_lt());
-        uint32_t bin = kBins - s;
+        const int bi = (int)B - 1 - (int)(c0 + lane);
+        const uint32_t s = bi >= 0 ? half_get(ws.cnt32, bi) : 0u;
+        const uint32_t peers = __match_any_sync(kFullMask, s ? s : 0x10000u + lane);
+        const uint32_t r = __popc(peers & lanemask_lt());
+        const uint32_t bin = kBins - s;
         if (s) {
-            ws.order[ws.binPos[bin] + r] = (uint16_t)bi;
-            ws.cur[bi] = ws.binKey[bin] + r * s;
+            const uint32_t j = ws.binPos[bin] + r, st = ws.binKey[bin] + r * s;
+            ws.order[j] = (uint16_t)bi;
+            ws.sched[j] = st | (s << 16);
+            ws.cur16[bi] = (uint16_t)st;
         }
         __syncwarp();
         if (s && lane == __ffs(peers) - 1) {
@@ -153,148 +305,86 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_search(SearchArgs a) {
     }
 
     // Keys into bucket order (redistribute_keys.comp:21-53, inside the partition).
+    const uint2 *lo = a.lowers + base;
+    uint2 *so = a.sorted + base;
+#pragma unroll 4
     for (uint32_t i = lane; i < ps; i += 32) {
-        uint32_t b = a.bkt[base + i];
-        uint32_t pos = atomicAdd(&ws.cur[b], 1u);
-        a.sorted[base + pos] = a.lowers[base + i];
+        uint32_t b = bk[i];
+        so[half_add(ws.cur32, b)] = lo[i];
     }
     __threadfence_block();
     __syncwarp();
 
+    // Pilot search (search.comp:126-175), next bucket's keys prefetched.
     const FastMod fm = FastMod::make(ps ? ps : 1);
     uint32_t k_lim = 0x80000000u / (ps ? ps : 1);
     if (k_lim > a.k_max) k_lim = a.k_max;
-
+    uint32_t sc_next = nonempty ? ws.sched[0] : 0u;
+    uint2 L_next = lane < (int)(sc_next >> 16) ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
     for (uint32_t j = 0; j < nonempty; j++) {
+        const uint32_t sc = sc_next;
+        const uint2 L = L_next;
         const uint32_t b = ws.order[j];
-        const uint32_t s = ws.cnt[b];
-        const uint32_t st = ws.cur[b] - s;
-        uint2 L[kMaxPerLane];
-        uint32_t H[kMaxPerLane];
-#pragma unroll
-        for (int r = 0; r < kMaxPerLane; r++) {
-            uint32_t i = lane + 32 * r;
-            L[r] = i < s ? a.sorted[base + st + i] : make_uint2(0, 0);
+        const uint32_t s = sc >> 16, st = sc & 0xFFFFu;
+        if (j + 1 < nonempty) {
+            sc_next = ws.sched[j + 1];
+            L_next = lane < (int)(sc_next >> 16) ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
         }
-        bool placed = false;
-        for (uint32_t k = 0; k < k_lim; k++) {
-            if (k == kDupCheckAt && s > 1) {
-                bool dupk = false;
-                for (uint32_t t = 0; t < s; t++) {
-                    uint2 kt = a.sorted[base + st + t];
-#pragma unroll
-                    for (int r = 0; r < kMaxPerLane; r++) {
-                        uint32_t i = lane + 32 * r;
-                        if (i < s && i > t && L[r].x == kt.x && L[r].y == kt.y) dupk = true;
-                    }
-                }
-                if (__any_sync(kFullMask, dupk)) {
-                    if (lane == 0) report_error(a.err, p, PHOBIC_ERR_DUPLICATE_KEY);
-                    return;
-                }
-            }
-            // Slots for this k (search.comp:44-70).
-#pragma unroll
-            for (int r = 0; r < kMaxPerLane; r++) {
-                uint32_t i = lane + 32 * r;
-                if (i < s) {
-                    H[r] = fm.mod(pilot_hash(L[r].x, L[r].y, k));
-                    ws.hs[i] = H[r];
-                }
-            }
-            bool dup = false;
-            if (s > 1) {
-                if (s <= 32) {
-                    uint32_t key = lane < (int)s ? H[0] : 0x80000000u | lane;
-                    uint32_t m = __match_any_sync(kFullMask, key);
-                    dup = __any_sync(kFullMask, lane < (int)s && __popc(m) > 1);
-                } else {
-                    bool d = false;
-#pragma unroll
-                    for (int r = 0; r < kMaxPerLane; r++) {
-                        uint32_t i = lane + 32 * r;
-                        if (i < s) {
-                            uint32_t bit = 1u << (H[r] & 31);
-                            if (atomicOr(&ws.scr[H[r] >> 5], bit) & bit) d = true;
-                        }
-                    }
-                    dup = __any_sync(kFullMask, d);
-#pragma unroll
-                    for (int r = 0; r < kMaxPerLane; r++) {
-                        uint32_t i = lane + 32 * r;
-                        if (i < s) ws.scr[H[r] >> 5] = 0;
-                    }
-                }
-            }
-            __syncwarp();
-            if (dup) continue;
-
-            // Smallest free offset (search.comp:72-103): lane L tests o in [w, w+32).
-            uint32_t o = 0xFFFFFFFFu;
-            for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
-                const uint32_t w = w0 + 32 * lane;
-                const bool live = w < ps;
-                const uint32_t wl = live ? w : 0u;
-                uint32_t bad = live ? 0u : kFullMask;
-                for (uint32_t i = 0; i < s; i++) {
-                    uint32_t x = ws.hs[i] + wl;
-                    if (x >= ps) x -= ps;
-                    uint32_t wi = x >> 5;
-                    bad |= __funnelshift_r(ws.occ[wi], ws.occ[wi + 1], x & 31);
-                    if ((i & 7) == 7 && __all_sync(kFullMask, bad == kFullMask)) break;
-                }
-                uint32_t valid = ~bad;
-                if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
-                uint32_t ball = __ballot_sync(kFullMask, valid != 0);
-                if (ball) {
-                    int f = __ffs(ball) - 1;
-                    uint32_t vf = __shfl_sync(kFullMask, valid, f);
-                    o = w0 + 32 * f + __ffs(vf) - 1;
-                    break;
-                }
-            }
-            if (o == 0xFFFFFFFFu) continue;
-
-            // Mark the slots (search.comp:113-117) and store the pilot (:122, :170-174).
-#pragma unroll
-            for (int r = 0; r < kMaxPerLane; r++) {
-                uint32_t i = lane + 32 * r;
-                if (i < s) {
-                    uint32_t q = H[r] + o;
-                    if (q >= ps) q -= ps;
-                    atomicOr(&ws.occ[q >> 5], 1u << (q & 31));
-                    if (q < 32) {
-                        uint32_t m = q + ps;
-                        atomicOr(&ws.occ[m >> 5], 1u << (m & 31));
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0) a.pilots[(size_t)b * a.partitions + p] = o + ps * k;
-            placed = true;
-            break;
-        }
-        if (!placed) {
-            if (lane == 0) report_error(a.err, p, PHOBIC_ERR_SEARCH_LIMIT);
-            return;
-        }
+        uint32_t pilot = 0;
+        const uint32_t st_code = s <= 32 ? place_small(ws.occ, L, s, ps, fm, k_lim, lane, &pilot)
+                                         : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
+        if (st_code != PHOBIC_OK) return st_code;
+        if (lane == 0) pil[(size_t)b * pstride] = pilot;
     }
+    return PHOBIC_OK;
 }
 
+}  // namespace
+
+size_t search_warp_smem(uint32_t buckets, uint32_t cap) { return 4 * warp_words(buckets, cap); }
+
 int search_warps_per_cta(uint32_t buckets, uint32_t cap) {
-    size_t per_warp = search_warp_smem(buckets, cap);
-    size_t fit = kSearchSmemLimit / per_warp;
+    if (cap > 65535 || buckets > 65535) return 0;
+    size_t fit = kSearchSmemLimit / search_warp_smem(buckets, cap);
     return (int)(fit < (size_t)kSearchWarps ? fit : (size_t)kSearchWarps);
 }
 
-cudaError_t launch_search(const SearchArgs &a, cudaStream_t st) {
-    if (a.partitions == 0) return cudaSuccess;
-    int warps = search_warps_per_cta(a.buckets, a.cap);
+__global__ void __launch_bounds__(kSearchWarps * 32, 4) k_search(SearchArgs a) {
+    extern __shared__ uint32_t smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const WarpSmem ws = carve(smem + (size_t)warp * warp_words(a.buckets, a.cap), a.buckets, a.cap);
+    for (;;) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(a.queue, 1u);
+        g = __shfl_sync(kFullMask, g, 0);
+        if (g >= a.M) break;
+        const uint32_t s = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, g);
+        if (fatal_before_search(*reinterpret_cast<volatile unsigned long long *>(&a.err[s]))) continue;
+        const SetDesc &d = a.sets[s];
+        const uint32_t p = g - d.part_base;
+        if (lane == 0 && d.part_off) {
+            const uint32_t g0 = a.G[d.part_base];
+            d.part_off[p] = a.G[g] - g0;
+            if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[g + 1] - g0;
+        }
+        const uint32_t code = search_partition(a, ws, d, g, p, lane);
+        if (code != PHOBIC_OK && lane == 0) report_error(&a.err[s], p, code);
+    }
+}
+
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st) {
+    if (a.M == 0) return cudaSuccess;
+    const int warps = search_warps_per_cta(a.buckets, a.cap);
     if (warps < 1) return cudaErrorInvalidValue;
-    size_t smem = (size_t)warps * search_warp_smem(a.buckets, a.cap);
+    const size_t smem = (size_t)warps * search_warp_smem(a.buckets, a.cap);
     cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    uint32_t grid = (a.partitions + warps - 1) / warps;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, warps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    uint64_t want = (a.M + warps - 1) / warps;
+    int grid = (int)std::min<uint64_t>(want, (uint64_t)per_sm * sm_count);
     k_search<<<grid, warps * 32, smem, st>>>(a);
     return cudaGetLastError();
 }

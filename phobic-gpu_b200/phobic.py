@@ -123,6 +123,7 @@ def _lib() -> C.CDLL:
         "phobic_ctx_destroy": (I32, [P]),
         "phobic_last_error": (C.c_char_p, [P]),
         "phobic_ctx_device_bytes": (U64, [P]),
+        "phobic_ctx_stream": (P, [P]),
         "phobic_build_bytes_needed": (U64, [C.POINTER(Keys), C.POINTER(Params)]),
         "phobic_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(Timings)]),
         "phobic_build_u64": (I32, [P, P, U64, C.POINTER(Params), P, P, C.POINTER(Timings)]),
@@ -289,6 +290,10 @@ class Context:
     def device_bytes(self) -> int:
         return int(_lib().phobic_ctx_device_bytes(self.handle))
 
+    def stream_handle(self) -> int:
+        """cudaStream_t of this context (all of its kernels run on it)."""
+        return int(_lib().phobic_ctx_stream(self.handle) or 0)
+
     def _result(self, cfg: MPHFconfig, n: int, out=None):
         parts = cfg.partitions(n)
         if out is not None:
@@ -349,3 +354,78 @@ class MPHFbuilder:
 
     def build(self, keys, out=None) -> BuildResult:
         return self.ctx.build(keys, self.config, out)
+
+
+# ------------------------------------------------------------------ batch and serving
+
+def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None = None):
+    """Build many key sets in one pass of the kernels; returns (results, statuses)."""
+    kss = [keyset(k, kind) for k in key_sets]
+    arr = (Keys * len(kss))(*[k.struct() for k in kss])
+    outs, res_structs = [], []
+    for ks in kss:
+        r, pil, off, parts = ctx._result(cfg, ks.n)
+        outs.append(BuildResult(pil, off, parts, cfg.bucketCountPerPartition))
+        res_structs.append(r)
+    rarr = (Result * len(kss))(*res_structs)
+    st = (C.c_int * len(kss))()
+    t = Timings()
+    rc = _lib().phobic_build_batch(ctx.handle, arr, len(kss), C.byref(cfg.params), rarr, st, C.byref(t))
+    for o in outs:
+        o.timings = t.as_dict()
+    if rc not in (OK,) and all(s == OK for s in st):
+        check(rc, ctx)
+    return outs, [int(s) for s in st]
+
+
+class Server:
+    """phobic_server: continuous-batching build server on one device."""
+
+    def __init__(self, device: int = 0, streams: int = 2, budget_bytes: int = 8 << 30, queue_capacity: int = 65536):
+        cfg = ServerConfig(device, streams, queue_capacity, budget_bytes)
+        h = C.c_void_p()
+        check(_lib().phobic_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h.value
+        self._live = {}
+
+    def submit(self, keys, cfg: MPHFconfig, kind: int | None = None) -> int:
+        ks = keyset(keys, kind)
+        parts = cfg.partitions(ks.n)
+        pil = np.zeros(max(cfg.bucketCountPerPartition * parts, 1), np.uint32)
+        off = np.zeros(parts + 1, np.uint32)
+        res = Result(0, pil.ctypes.data, off.ctypes.data)
+        k = ks.struct()
+        t = C.c_uint64()
+        check(_lib().phobic_server_submit(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(t)))
+        self._live[t.value] = (ks, k, res, BuildResult(pil[: cfg.bucketCountPerPartition * parts], off, parts,
+                                                        cfg.bucketCountPerPartition))
+        return int(t.value)
+
+    def wait(self, ticket: int, timeout_ms: int = 600_000) -> tuple[int, BuildResult]:
+        st = C.c_int()
+        check(_lib().phobic_server_wait(self.handle, ticket, timeout_ms, C.byref(st)))
+        return int(st.value), self._live.pop(ticket)[3]
+
+    def poll(self, ticket: int) -> tuple[bool, int]:
+        done, st = C.c_int(), C.c_int()
+        check(_lib().phobic_server_poll(self.handle, ticket, C.byref(done), C.byref(st)))
+        return bool(done.value), int(st.value)
+
+    def drain(self, timeout_ms: int = 600_000) -> None:
+        check(_lib().phobic_server_drain(self.handle, timeout_ms))
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(_lib().phobic_server_stats_get(self.handle, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in s._fields_}
+
+    def close(self) -> None:
+        if self.handle:
+            _lib().phobic_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

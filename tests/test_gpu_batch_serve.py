@@ -1,0 +1,105 @@
+"""Batched builds and the build server through the C ABI: every set's result
+equals the plain build of that set alone (bit-exact pilots and offsets), and
+every set is a bijection."""
+import numpy as np
+import pytest
+
+import keygen
+import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle(keys4, cfg):
+    r = O.build(keys4, cfg.partitionSize, cfg.bucketCountPerPartition, cfg.getFulcs())
+    assert r["status"] == 0
+    return r
+
+
+def test_batch_equals_plain_builds(phobic, ctx):
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    sizes = [0, 1, 5, 2047, 2048, 2049, 10_000, 1000, 77_777, 3]
+    sets = [keygen.splitmix64(100 + i, n) for i, n in enumerate(sizes)]
+    outs, st = phobic.build_batch(ctx, sets, cfg)
+    assert st == [0] * len(sets)
+    for keys, got in zip(sets, outs):
+        want = oracle(O.hash_keys(keys, "u64"), cfg)
+        assert (got.pilots == want["pilots"]).all()
+        assert (got.partition_offsets == want["offsets"]).all()
+        if len(keys):
+            assert ctx.verify(keys, cfg, got) == 0
+
+
+def test_batch_many_small_sets_log_uniform(phobic, ctx):
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    sizes = keygen.set_sizes(4, 300, 1000, 200_000)
+    sets = [keygen.splitmix64(10_000 + i, int(n)) for i, n in enumerate(sizes)]
+    outs, st = phobic.build_batch(ctx, sets, cfg)
+    assert all(s == 0 for s in st)
+    for i in range(0, len(sets), 37):
+        want = oracle(O.hash_keys(sets[i], "u64"), cfg)
+        assert (outs[i].pilots == want["pilots"]).all()
+    for keys, got in zip(sets, outs):
+        assert ctx.verify(keys, cfg, got) == 0
+
+
+def test_batch_strings_and_mixed_kinds(phobic, ctx):
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    s1 = keygen.strings(31, 5000)
+    s2 = keygen.strings(32, 12_000)
+    u = keygen.splitmix64(33, 9000)
+    outs, st = phobic.build_batch(ctx, [s1, u, s2], cfg)
+    assert st == [0, 0, 0]
+    for keys, kind, got in ((s1, "strings", outs[0]), (u, "u64", outs[1]), (s2, "strings", outs[2])):
+        want = oracle(O.hash_keys(keys, kind), cfg)
+        assert (got.pilots == want["pilots"]).all()
+
+
+def test_batch_reports_per_set_errors(phobic, ctx):
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    good = keygen.splitmix64(40, 5000)
+    dup = keygen.splitmix64(41, 5000)
+    dup[7] = dup[3]
+    outs, st = phobic.build_batch(ctx, [good, dup, good.copy()], cfg)
+    assert st[0] == 0 and st[2] == 0 and st[1] == phobic.ERR_DUPLICATE_KEY
+    assert ctx.verify(good, cfg, outs[0]) == 0 and ctx.verify(good, cfg, outs[2]) == 0
+
+
+def test_server_results_equal_alone(phobic):
+    cfg = phobic.MPHFconfig(7.0, 2048)
+    rng = np.random.default_rng(5)
+    reqs = []
+    for i in range(40):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(3e5))))
+        reqs.append(keygen.strings(500 + i, n) if i % 3 == 2 else keygen.splitmix64(500 + i, n))
+    with phobic.Server(0, streams=3, budget_bytes=4 << 30) as srv:
+        tickets = [srv.submit(k, cfg) for k in reqs]
+        results = [srv.wait(t) for t in tickets]
+        stats = srv.stats()
+    assert stats["completed"] == len(reqs) and stats["failed"] == 0
+    assert stats["p50_ms"] > 0 and stats["p99_ms"] >= stats["p50_ms"]
+    assert stats["peak_bytes"] <= 4 << 30
+    with phobic.Context(0) as alone:
+        for i, (keys, (st, got)) in enumerate(zip(reqs, results)):
+            assert st == 0
+            ref = alone.build(keys, cfg)
+            assert (got.pilots == ref.pilots).all() and (got.partition_offsets == ref.partition_offsets).all()
+
+
+def test_server_budget_admission(phobic):
+    cfg = phobic.MPHFconfig(7.0, 2048)
+    big = keygen.splitmix64(9, 2_000_000)
+    small = keygen.splitmix64(10, 10_000)
+    need = phobic.lib().phobic_build_bytes_needed(
+        __import__("ctypes").byref(phobic.keyset(big).struct()), __import__("ctypes").byref(cfg.params))
+    with phobic.Server(0, streams=2, budget_bytes=need + (1 << 20)) as srv:
+        with pytest.raises(phobic.PhobicError) as e:
+            srv.submit(keygen.splitmix64(11, 3_000_000), cfg)
+        assert e.value.status == phobic.ERR_BUDGET
+        t1 = srv.submit(big, cfg)
+        t2 = srv.submit(big.copy(), cfg)
+        t3 = srv.submit(small, cfg)
+        for t in (t1, t2, t3):
+            st, _ = srv.wait(t)
+            assert st == 0
+        assert srv.stats()["peak_bytes"] <= need + (1 << 20)
