@@ -170,6 +170,15 @@ phobic_status check_keys(const phobic_keys *keys, std::string *err) {
     if (keys->n > 0xFFFFFFFFull) return bad("more than 2^32-1 keys (the reference's uint32 size, mphf_builder.h:56)");
     if (keys->kind == PHOBIC_KEYS_STRINGS && keys->n && !keys->offsets) return bad("strings need offsets");
     if (keys->kind != PHOBIC_KEYS_STRINGS && keys->n && !keys->data) return bad("null key data");
+    if (keys->on_device && keys->n) {
+        // The kernels read u64 keys and 16-byte records as 8-byte words, Keys as 4-byte
+        // words, and string offsets as 8-byte words.
+        uintptr_t d = reinterpret_cast<uintptr_t>(keys->data), o = reinterpret_cast<uintptr_t>(keys->offsets);
+        if ((keys->kind == PHOBIC_KEYS_U64 || keys->kind == PHOBIC_KEYS_BYTES16) && (d & 7))
+            return bad("device keys must be 8-byte aligned");
+        if (keys->kind == PHOBIC_KEYS_PREHASHED && (d & 3)) return bad("device Key records must be 4-byte aligned");
+        if (keys->kind == PHOBIC_KEYS_STRINGS && (o & 7)) return bad("device string offsets must be 8-byte aligned");
+    }
     return PHOBIC_OK;
 }
 
@@ -235,6 +244,10 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         const phobic_result &r = results[s];
         if (!r.partition_offsets || (!r.pilots && sets[s].n)) {
             if (err) *err = "null result arrays";
+            return PHOBIC_ERR_INVALID;
+        }
+        if (r.on_device && ((reinterpret_cast<uintptr_t>(r.pilots) | reinterpret_cast<uintptr_t>(r.partition_offsets)) & 3)) {
+            if (err) *err = "device result arrays must be 4-byte aligned";
             return PHOBIC_ERR_INVALID;
         }
         N += sets[s].n;

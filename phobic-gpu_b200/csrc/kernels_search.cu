@@ -40,17 +40,24 @@ constexpr uint32_t kNone = 0xFFFFFFFFu;
 __host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (cap + 31) / 32 + 2; }
 __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B + 1) / 2; }
 
-// Per-warp shared memory, in 32-bit words:
+// Per-warp shared memory, in 32-bit words; every warp's region starts on a
+// 16-byte boundary (its size is rounded up to 4 words) and the union comes first,
+// so the uint2 staging array kl is 8-byte aligned:
+//   union of
+//     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
+//     search phase:  hs [256] slots, kl uint2[256] keys of a large bucket
 //   sched [B]        search schedule, in search order: start | size << 16
 //   order [B/2]      bucket id (u16) in search order
 //   occ   [OW]       occupied slots, bits [ps, ps+32) mirror [0, 32)
 //   scr   [OW]       collision scratch of large buckets
-//   union of
-//     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
-//     search phase:  hs [256] slots, kl uint2[256] keys of a large bucket
-__host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
+__host__ __device__ __forceinline__ size_t union_words(uint32_t B) {
     size_t prep = 2 * (size_t)half_words(B) + 512, search = 256 + 512;
-    return (size_t)B + half_words(B) + 2 * (size_t)occ_words(cap) + (prep > search ? prep : search);
+    return prep > search ? prep : search;
+}
+
+__host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
+    size_t w = union_words(B) + (size_t)B + half_words(B) + 2 * (size_t)occ_words(cap);
+    return (w + 3) & ~size_t(3);
 }
 
 struct WarpSmem {
@@ -66,18 +73,17 @@ struct WarpSmem {
 
 __device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap) {
     WarpSmem m;
-    m.sched = w;
-    m.order = reinterpret_cast<uint16_t *>(w + B);
-    m.occ = w + B + half_words(B);
-    m.scr = m.occ + occ_words(cap);
-    uint32_t *u = m.scr + occ_words(cap);
-    m.cnt32 = u;
-    m.cur32 = u + half_words(B);
+    m.cnt32 = w;
+    m.cur32 = w + half_words(B);
     m.cur16 = reinterpret_cast<uint16_t *>(m.cur32);
-    m.binPos = u + 2 * half_words(B);
+    m.binPos = w + 2 * half_words(B);
     m.binKey = m.binPos + 256;
-    m.hs = u;
-    m.kl = reinterpret_cast<uint2 *>(u + 256);
+    m.hs = w;
+    m.kl = reinterpret_cast<uint2 *>(w + 256);
+    m.sched = w + union_words(B);
+    m.order = reinterpret_cast<uint16_t *>(m.sched + B);
+    m.occ = m.sched + B + half_words(B);
+    m.scr = m.occ + occ_words(cap);
     return m;
 }
 
