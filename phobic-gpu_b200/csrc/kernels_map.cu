@@ -40,6 +40,10 @@ struct SetCache {
 
 }  // namespace
 
+// Each thread takes kUnroll keys per iteration, kStride apart, so that their
+// loads and atomics are in flight together; the warp's loads stay coalesced.
+constexpr int kUnroll = 4;
+
 template <int KIND, bool SCATTER>
 __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     __shared__ uint32_t sf[kFulcrums];
@@ -51,29 +55,46 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     SetCache c;
     uint32_t bad_set = 0xFFFFFFFFu;
-    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < a.total_keys; g += stride) {
-        uint32_t gp, b, l1, l2;
-        if constexpr (kReadMapped) {
-            uint4 r = a.mapped[g];
-            gp = r.x, b = r.y, l1 = r.z, l2 = r.w;
-        } else {
-            c.locate(a, g);
-            Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
-            gp = c.part_base + partition_of(k.partitioner, c.partitions);
-            b = bucket_of(k.bucketer, sf);
-            l1 = k.lower1, l2 = k.lower2;
-            if (!SCATTER) {
-                if (b >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = c.s;
-                if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+    for (uint64_t g0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g0 < a.total_keys; g0 += kUnroll * stride) {
+        uint32_t gp[kUnroll], b[kUnroll], l1[kUnroll], l2[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const uint64_t g = g0 + u * stride;
+            gp[u] = 0xFFFFFFFFu;
+            if (g >= a.total_keys) continue;
+            if constexpr (kReadMapped) {
+                uint4 r = a.mapped[g];
+                gp[u] = r.x, b[u] = r.y, l1[u] = r.z, l2[u] = r.w;
+            } else {
+                c.locate(a, g);
+                Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
+                gp[u] = c.part_base + partition_of(k.partitioner, c.partitions);
+                b[u] = bucket_of(k.bucketer, sf);
+                l1[u] = k.lower1, l2[u] = k.lower2;
+                if (!SCATTER) {
+                    if (b[u] >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = c.s;
+                    if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+                }
             }
         }
         if constexpr (SCATTER) {
-            uint32_t slot = atomicAdd(&a.counts[gp], 1u);
-            a.lowers[slot] = make_uint2(l1, l2);
-            a.bkt[slot] = (uint16_t)b;
+            uint32_t slot[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++)
+                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&a.counts[gp[u]], 1u);
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                if (gp[u] == 0xFFFFFFFFu) continue;
+                a.lowers[slot[u]] = make_uint2(l1[u], l2[u]);
+                a.bkt[slot[u]] = (uint16_t)b[u];
+            }
         } else {
-            atomicAdd(&a.counts[gp], 1u);
-            if (KIND == PHOBIC_KEYS_STRINGS) a.mapped[g] = make_uint4(gp, b, l1, l2);
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                if (gp[u] == 0xFFFFFFFFu) continue;
+                atomicAdd(&a.counts[gp[u]], 1u);
+                if (KIND == PHOBIC_KEYS_STRINGS) a.mapped[g0 + u * stride] = make_uint4(gp[u], b[u], l1[u], l2[u]);
+            }
         }
     }
     if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);

@@ -20,11 +20,14 @@
 // partitions of very different cost (and of different key sets in a batched
 // build) spread over the SMs without CTA-level tail imbalance.
 //
-// Offset search: the occupancy bitmap keeps a copy of its first 32 bits after
-// bit ps, so the 32-bit window that starts at any slot < ps reads circularly
-// with one funnel shift.  Lane L tests offsets [w, w+32), w = w0 + 32 L, by
-// OR-ing the windows of all keys; a warp covers 1024 offsets per round and the
-// first lane with a free window holds the smallest valid offset.
+// Offset search: the occupancy bitmap is stored twice in a row (bits [ps, 2 ps)
+// repeat bits [0, ps)), so the 32 slots (h + o) mod ps, o in [w, w + 32), are the
+// bits [h + w, h + w + 32) of the doubled bitmap for any slot h < ps and w < ps,
+// read with two loads and one funnel shift.  Lane L tests offsets [w, w + 32),
+// w = w0 + 32 L, by OR-ing the windows of all keys of the bucket; a warp covers
+// 1024 offsets per round and the first lane with a free window holds the
+// smallest valid offset.  Because w is a multiple of 32, the word index of a
+// window is (h >> 5) + (w >> 5) and its bit shift is h & 31 for every lane.
 //
 // Buckets of at most 32 keys (nearly all of them) keep one key per lane in
 // registers, test collisions with __match_any_sync and broadcast slots with
@@ -36,8 +39,13 @@ namespace phobicb200 {
 namespace {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kHsWords = 260;  // even, so kl after it stays 8-byte aligned
 
-__host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (cap + 31) / 32 + 2; }
+// Occupancy bitmap of a partition of at most cap slots, stored twice in a row
+// (bits [ps, 2 ps) repeat bits [0, ps)) plus one spare word.
+__host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (2 * cap + 31) / 32 + 2; }
+// Collision scratch of large buckets: one bit per slot.
+__host__ __device__ __forceinline__ uint32_t scr_words(uint32_t cap) { return (cap + 31) / 32 + 1; }
 __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B + 1) / 2; }
 
 // Per-warp shared memory, in 32-bit words; every warp's region starts on a
@@ -45,18 +53,19 @@ __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B 
 // so the uint2 staging array kl is 8-byte aligned:
 //   union of
 //     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
-//     search phase:  hs [256] slots, kl uint2[256] keys of a large bucket
+//     search phase:  hs [260] slots (256 keys + 3 padding copies of slot 0),
+//                    kl uint2[256] keys of a large bucket
 //   sched [B]        search schedule, in search order: start | size << 16
 //   order [B/2]      bucket id (u16) in search order
-//   occ   [OW]       occupied slots, bits [ps, ps+32) mirror [0, 32)
-//   scr   [OW]       collision scratch of large buckets
+//   occ   [OW]       occupied slots, bits [ps, 2 ps) mirror [0, ps)
+//   scr   [SW]       collision scratch of large buckets
 __host__ __device__ __forceinline__ size_t union_words(uint32_t B) {
-    size_t prep = 2 * (size_t)half_words(B) + 512, search = 256 + 512;
+    size_t prep = 2 * (size_t)half_words(B) + 512, search = kHsWords + 512;
     return prep > search ? prep : search;
 }
 
 __host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
-    size_t w = union_words(B) + (size_t)B + half_words(B) + 2 * (size_t)occ_words(cap);
+    size_t w = union_words(B) + (size_t)B + half_words(B) + (size_t)occ_words(cap) + scr_words(cap);
     return (w + 3) & ~size_t(3);
 }
 
@@ -79,7 +88,7 @@ __device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap)
     m.binPos = w + 2 * half_words(B);
     m.binKey = m.binPos + 256;
     m.hs = w;
-    m.kl = reinterpret_cast<uint2 *>(w + 256);
+    m.kl = reinterpret_cast<uint2 *>(w + kHsWords);
     m.sched = w + union_words(B);
     m.order = reinterpret_cast<uint16_t *>(m.sched + B);
     m.occ = m.sched + B + half_words(B);
@@ -104,58 +113,51 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
 
 __device__ __forceinline__ void mark(uint32_t *occ, uint32_t q, uint32_t ps) {
     atomicOr(&occ[q >> 5], 1u << (q & 31));
-    if (q < 32) {
-        uint32_t m = q + ps;
-        atomicOr(&occ[m >> 5], 1u << (m & 31));
-    }
+    const uint32_t m = q + ps;
+    atomicOr(&occ[m >> 5], 1u << (m & 31));
 }
 
-// Smallest free offset for slots held one per lane (lanes < s).
-__device__ __forceinline__ uint32_t offset_small(const uint32_t *occ, uint32_t h, uint32_t s, uint32_t ps, int lane) {
+__device__ __forceinline__ uint32_t lds32(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds32_next(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1+4];" : "=r"(v) : "r"(addr));
+    return v;
+}
+
+// Smallest free offset in rounds of 1024 (see the offset search above).  Keys are
+// consumed in unrolled groups of 4; SlotOf(i) returns key i's slot for i < s + 3,
+// where slots past the last key repeat key 0 (OR is idempotent).  A round stops
+// early once every lane's window holds an occupied slot.  The bitmap is addressed
+// through 32-bit shared-memory addresses: lane base + 4 * (slot >> 5).
+template <typename SlotOf>
+__device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, uint32_t s, uint32_t ps, int lane,
+                                                      SlotOf slot_of) {
+    const uint32_t occ_sa = (uint32_t)__cvta_generic_to_shared(occ);
     for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
         const uint32_t w = w0 + 32 * lane;
         const bool live = w < ps;
-        const uint32_t wl = live ? w : 0u;
+        const uint32_t base = occ_sa + (live ? (w >> 3) : 0u);
         uint32_t bad = live ? 0u : kFullMask;
-#pragma unroll 4
-        for (uint32_t i = 0; i < s; i++) {
-            uint32_t x = __shfl_sync(kFullMask, h, i) + wl;
-            if (x >= ps) x -= ps;
-            bad |= __funnelshift_r(occ[x >> 5], occ[(x >> 5) + 1], x & 31);
-        }
-        uint32_t valid = ~bad;
-        if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
-        uint32_t ball = __ballot_sync(kFullMask, valid != 0);
-        if (ball) {
-            int f = __ffs(ball) - 1;
-            return w0 + 32 * f + __ffs(__shfl_sync(kFullMask, valid, f)) - 1;
-        }
-    }
-    return kNone;
-}
-
-// Smallest free offset for slots staged in shared memory (any s <= 256).
-__device__ __forceinline__ uint32_t offset_large(const uint32_t *occ, const uint32_t *hs, uint32_t s, uint32_t ps,
-                                                 int lane) {
-    for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
-        const uint32_t w = w0 + 32 * lane;
-        const bool live = w < ps;
-        const uint32_t wl = live ? w : 0u;
-        uint32_t bad = live ? 0u : kFullMask;
-        for (uint32_t i = 0; i < s; i += 8) {
-            uint32_t e = min(s, i + 8);
-            for (uint32_t t = i; t < e; t++) {
-                uint32_t x = hs[t] + wl;
-                if (x >= ps) x -= ps;
-                bad |= __funnelshift_r(occ[x >> 5], occ[(x >> 5) + 1], x & 31);
+        for (uint32_t i = 0; i < s; i += 4) {
+            uint32_t h[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) h[u] = slot_of(i + u);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const uint32_t a = base + ((h[u] >> 5) << 2);
+                bad |= __funnelshift_r(lds32(a), lds32_next(a), h[u]);
             }
             if (__all_sync(kFullMask, bad == kFullMask)) break;
         }
         uint32_t valid = ~bad;
         if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
-        uint32_t ball = __ballot_sync(kFullMask, valid != 0);
+        const uint32_t ball = __ballot_sync(kFullMask, valid != 0);
         if (ball) {
-            int f = __ffs(ball) - 1;
+            const int f = __ffs(ball) - 1;
             return w0 + 32 * f + __ffs(__shfl_sync(kFullMask, valid, f)) - 1;
         }
     }
@@ -180,7 +182,8 @@ __device__ __forceinline__ uint32_t place_small(uint32_t *occ, uint2 L, uint32_t
             uint32_t m = __match_any_sync(kFullMask, h);
             if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
         }
-        const uint32_t o = offset_small(occ, h, s, ps, lane);
+        const uint32_t hp = __shfl_sync(kFullMask, h, mine ? lane : 0);
+        const uint32_t o = first_free_offset(occ, s, ps, lane, [&](uint32_t j) { return __shfl_sync(kFullMask, hp, j); });
         if (o == kNone) continue;
         if (mine) {
             uint32_t q = h + o;
@@ -219,7 +222,10 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
         for (uint32_t i = lane; i < s; i += 32) ws.scr[ws.hs[i] >> 5] = 0;
         __syncwarp();
         if (dup) continue;
-        const uint32_t o = offset_large(ws.occ, ws.hs, s, ps, lane);
+        if (lane < 3) ws.hs[s + lane] = ws.hs[0];
+        __syncwarp();
+        const uint32_t *hs = ws.hs;
+        const uint32_t o = first_free_offset(ws.occ, s, ps, lane, [&](uint32_t j) { return hs[j]; });
         if (o == kNone) continue;
         for (uint32_t i = lane; i < s; i += 32) {
             uint32_t q = ws.hs[i] + o;
@@ -244,7 +250,8 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     const size_t pstride = d.partitions;
 
     for (uint32_t i = lane; i < half_words(B); i += 32) ws.cnt32[i] = 0;
-    for (uint32_t i = lane; i < ow; i += 32) ws.occ[i] = 0, ws.scr[i] = 0;
+    for (uint32_t i = lane; i < ow; i += 32) ws.occ[i] = 0;
+    for (uint32_t i = lane; i < scr_words(a.cap); i += 32) ws.scr[i] = 0;
     for (uint32_t i = lane; i < 512; i += 32) ws.binPos[i] = 0;
     __syncwarp();
 
