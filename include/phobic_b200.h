@@ -169,6 +169,29 @@ PHOBIC_API phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys,
 PHOBIC_API phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
                                  const phobic_result *result, uint32_t *keys4, uint32_t *bucket_sizes);
 
+/* ------------------------------------------------------------------ no allocation
+ * phobic_build_noalloc has no counterpart in the reference.  It is the plain build
+ * for callers that cannot allocate device memory: a host framework that owns the
+ * whole device memory pool and only hands out buffers it sized itself, a latency-
+ * critical path that cannot pay cudaMalloc's implicit synchronisation, or a plugin
+ * host that forbids allocation inside its callbacks.  It allocates nothing (no
+ * cudaMalloc, cudaFree, pinned memory, stream or event creation); every scratch byte
+ * comes from one static device array of about 20 MiB that each GPU loading this
+ * library holds until the process exits.
+ *   - keys: device-resident, kind U64, BYTES16 or PREHASHED, at most 1,048,576 keys
+ *     in at most 65,536 partitions; larger builds return PHOBIC_ERR_BUDGET, other
+ *     unsupported inputs PHOBIC_ERR_INVALID.
+ *   - result: device arrays (on_device = 1), as for phobic_build.
+ *   - stream: the cudaStream_t to run on (NULL = legacy default stream); the call
+ *     returns after that stream has drained, with the build's status.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) for that device; make that first call before any stream
+ * capture.  All calls share the array and it keeps the last call's contents (the
+ * call clears what must start at zero), so calls whose work overlaps on the GPU
+ * race with each other and must not be made. */
+PHOBIC_API phobic_status phobic_build_noalloc(const phobic_keys *keys, const phobic_params *params,
+                                              const phobic_result *result, void *stream);
+
 /* ------------------------------------------------------------------ serving
  * A build server: a request loop that admits key sets as they arrive against a
  * device-memory budget, keeps buffers resident, overlaps admitted requests on
