@@ -1,0 +1,82 @@
+// The MPHF container and query (reference: include/phobicGpu/mphf.hpp:20-97).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "config.hpp"
+#include "encoders.hpp"
+
+namespace phobicgpu {
+
+template <typename PilotEncoder, typename PartitionOffsetEncoder, typename Hasher>
+class MPHF {
+  private:
+    std::vector<uint32_t> fulcs;
+    uint32_t partitions = 0;
+    PilotEncoder pilots;
+    PartitionOffsetEncoder partitionOffsets;
+
+    // Bucket by the 64-bit fulcrum interpolation (mphf.hpp:42-49).
+    uint64_t getBucket(uint32_t bucketer) const { return phobicb200::bucket_of_query(bucketer, fulcs.data()); }
+
+  public:
+    PilotEncoder &getPilotEncoder() { return pilots; }
+    PartitionOffsetEncoder &getPartitionOffsetEncoder() { return partitionOffsets; }
+    uint32_t getPartitions() const { return partitions; }
+
+    constexpr static bool noHash() { return std::is_same_v<Hasher, nohash>; }
+
+    template <typename keyType>
+    static inline Key initialHash(const keyType &keyRaw) {
+        return Hasher::hash(keyRaw);
+    }
+
+    // Encodes the serialized pilot layout: pilots[b * partitions + p] and the
+    // exclusive partition offsets [partitions + 1] (mphf.hpp:65-75).
+    void setData(const std::vector<uint32_t> &pilot_values, std::vector<uint32_t> &offsets, uint32_t parts,
+                 MPHFconfig config) {
+        fulcs = config.getFulcs();
+        partitions = parts;
+        partitionOffsets.encode(offsets.begin(), config.partitionSize, parts + 1);
+        pilots.encode(pilot_values.begin(), parts, config.bucketCountPerPartition);  // columns in parallel
+    }
+
+    // Slot of a key in [0, n) (mphf.hpp:77-86).
+    template <typename keyType>
+    inline uint32_t operator()(const keyType &keyRaw) const {
+        const Key key = initialHash(keyRaw);
+        const uint64_t partition = (uint64_t(key.partitioner) * uint64_t(partitions)) >> 32;
+        const uint64_t bucket = getBucket(key.bucketer);
+        const uint32_t pilot = uint32_t(pilots.access(partition, bucket));
+        const uint32_t offset = uint32_t(partitionOffsets.access(partition));
+        const uint32_t size = uint32_t(partitionOffsets.access(partition + 1)) - offset;
+        return offset + phobicb200::slot_of(pilot, key.lower1, key.lower2, size);
+    }
+
+    float getBitsPerKey() const {
+        return float(pilots.num_bits() + partitionOffsets.num_bits() + 32 * fulcs.size() + 32 * partitions) /
+               float(partitionOffsets.access(partitions));
+    }
+
+    std::string getResultLine() {
+        const double n = float(partitionOffsets.access(partitions));
+        return "total_bits=" + std::to_string(getBitsPerKey()) + " pilot_bits=" + std::to_string(pilots.num_bits() / n) +
+               " offsets_bits=" + std::to_string(partitionOffsets.num_bits() / n);
+    }
+
+    // Serialisation of the whole function (the reference's MPHF has none): the
+    // partition count, the fulcrum table, then the two encoders in their own
+    // visit order.
+    template <typename Visitor>
+    void visit(Visitor &visitor) {
+        visitor.visit(partitions);
+        visitor.visit(fulcs);
+        pilots.visit(visitor);
+        partitionOffsets.visit(visitor);
+    }
+};
+
+}  // namespace phobicgpu
