@@ -21,6 +21,7 @@ collective on the data path); rank 0 prints.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -68,7 +69,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -193,6 +194,7 @@ def run_ours(args) -> None:
     dp = torch.empty(parts * B, dtype=torch.int32, device="cuda")
     do = torch.empty(parts + 1, dtype=torch.int32, device="cuda")
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    clocks = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         ctx.build(dk, cfg, out=(dp, do))
     torch.cuda.synchronize()
@@ -200,14 +202,13 @@ def run_ours(args) -> None:
         pg.barrier()
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     search_ms = []
-    with ClockSampler(local) as clocks:
-        torch.cuda.synchronize()
-        t_start.record(stream)
-        for _ in range(args.steps):
-            r = ctx.build(dk, cfg, out=(dp, do))
-            search_ms.append(r.timings["search"])
-        t_end.record(stream)
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    t_start.record(stream)
+    for _ in range(args.steps):
+        r = ctx.build(dk, cfg, out=(dp, do))
+        search_ms.append(r.timings["search"])
+    t_end.record(stream)
+    torch.cuda.synchronize()
     dev_ms = t_start.elapsed_time(t_end)
     stage = dict(r.timings)
     if pg:
@@ -235,12 +236,19 @@ def run_ours(args) -> None:
         r2 = ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
         e2e_wall.append(time.perf_counter() - t0)
         e2e_dev.append(r2.timings["total"])
+    clocks.__exit__(None, None, None)
     e2e_ms = 1e3 * sum(e2e_wall) / len(e2e_wall)
     if pg:
         t = torch.tensor([e2e_ms], device="cuda")
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_ms = float(t.item())
     same = bool((hp.numpy() == dp.cpu().numpy()).all())
+
+    # ---- host encoding of the result (Mphf::setData), C2's encoder: interleaved dictionary + diff compact
+    built = phobic.BuildResult(hp.numpy().view(np.uint32), ho.numpy().view(np.uint32), parts, B)
+    t0 = time.perf_counter()
+    blob, bits_per_key = phobic.encode(built, cfg, "interleaved_dictionary", "diff")
+    encode_ms = 1e3 * (time.perf_counter() - t0)
 
     if rank != 0:
         ctx.close()
@@ -274,6 +282,9 @@ def run_ours(args) -> None:
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "bytes_per_key": K4_BYTES_PER_KEY,
                      "launch_ms": k4_ms},
+        "encoding": {"encoder": "interleaved<dictionary> + diff<compact>", "ms": encode_ms,
+                     "bits_per_key": bits_per_key, "bytes": len(blob), "host_threads": os.cpu_count(),
+                     "e2e_with_encoding_mkeys_s": world * n / ((e2e_ms + encode_ms) / 1e3) / 1e6},
         "cpu_baseline": base,
         "clocks": clocks.summary(),
     }
@@ -282,6 +293,204 @@ def run_ours(args) -> None:
     if pg:
         pg.barrier()
         pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ other workloads
+
+def _plain_device_ms(ctx, keys_dev, cfg, steps, warmup, torch, kind=None):
+    """Mean device time of a plain build with device-resident keys and results (CUDA events)."""
+    import phobic
+
+    ks = phobic.keyset(keys_dev, kind)
+    parts = cfg.partitions(ks.n)
+    dp = torch.empty(max(parts * cfg.bucketCountPerPartition, 1), dtype=torch.int32, device="cuda")
+    do = torch.empty(parts + 1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    for _ in range(warmup):
+        r = ctx.build(ks, cfg, out=(dp, do))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(steps):
+        r = ctx.build(ks, cfg, out=(dp, do))
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, r.timings, phobic.BuildResult(dp, do, parts, cfg.bucketCountPerPartition)
+
+
+def run_plain_workload(args, name, lam, P, make_keys, describe) -> None:
+    """C1 / C3: a plain build of one key set (device-resident value, host e2e)."""
+    import torch
+
+    import phobic
+
+    cfg = phobic.MPHFconfig(lam, P)
+    host_keys, kind = make_keys()
+    ctx = phobic.Context(0)
+    if kind == phobic.KEYS_STRINGS:
+        data, offs = host_keys
+        dev = (torch.from_numpy(data).cuda(), torch.from_numpy(offs.view(np.int64)).cuda())
+        pinned = (torch.from_numpy(data).pin_memory(), torch.from_numpy(offs.view(np.int64)).pin_memory())
+        n = len(offs) - 1
+        dev_ks = phobic.KeySet(kind, n, dev[0], dev[1], True)
+        host_ks = phobic.KeySet(kind, n, pinned[0].data_ptr(), pinned[1].data_ptr())
+        h2d = int(offs[-1]) + 8 * (n + 1)
+    else:
+        n = len(host_keys)
+        dev_ks = phobic.KeySet(kind, n, torch.from_numpy(host_keys.view(np.int64)).cuda(), None, True)
+        pinned = torch.from_numpy(host_keys.view(np.int64)).pin_memory()
+        host_ks = phobic.KeySet(kind, n, pinned.data_ptr())
+        h2d = 8 * n
+    ms, stages, built = _plain_device_ms(ctx, dev_ks, cfg, args.steps, args.warmup, torch)
+    bad = ctx.verify(dev_ks, cfg, built)
+    parts = cfg.partitions(n)
+    hp = torch.empty(max(parts * cfg.bucketCountPerPartition, 1), dtype=torch.int32).pin_memory()
+    ho = torch.empty(parts + 1, dtype=torch.int32).pin_memory()
+    ctx.build(host_ks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
+    wall = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.build(host_ks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
+        wall.append(time.perf_counter() - t0)
+    e2e_ms = 1e3 * statistics.mean(wall)
+    print(json.dumps({
+        "workload": name, "metric": "Mkeys/s MPHF build", "value": n / ms / 1e3, "unit": "Mkeys/s",
+        "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup, "config": describe, "n_keys": n,
+        "stages_ms": {k: round(v, 4) for k, v in stages.items() if k != "kernels"}, "bijection_bad": bad,
+        "e2e": {"value": n / e2e_ms / 1e3, "unit": "Mkeys/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 4 * (parts * cfg.bucketCountPerPartition + parts + 1)},
+    }), flush=True)
+    ctx.close()
+
+
+def run_c4(args) -> None:
+    """Batched build: 4096 u64 key sets, sizes log-uniform in [1K, 4M] (seed 4), lambda 6,
+    P 2048, all sets in one batch vs 4096 plain sequential builds on the same GPU."""
+    import torch
+
+    import keygen
+    import phobic
+
+    lam, P = 6.0, 2048
+    cfg = phobic.MPHFconfig(lam, P)
+    B = cfg.bucketCountPerPartition
+    sizes = keygen.set_sizes(4, args.c4_sets, 1000, 4 << 20)
+    total = int(sizes.sum())
+    keys = keygen.splitmix64_cuda(4, total)  # one stream split into the sets: unique keys
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    sets = [keys[int(starts[i]):int(starts[i + 1])] for i in range(len(sizes))]
+    outs = []
+    for n in sizes:
+        parts = cfg.partitions(int(n))
+        outs.append((torch.empty(parts * B, dtype=torch.int32, device="cuda"),
+                     torch.empty(parts + 1, dtype=torch.int32, device="cuda")))
+    ctx = phobic.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    phobic.build_batch(ctx, sets, cfg, outs_in=outs)  # warm-up: grows the arena
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res, st = phobic.build_batch(ctx, sets, cfg, outs_in=outs)
+    batch_wall = time.perf_counter() - t0
+    batch_dev = res[0].timings["total"]
+    assert all(x == 0 for x in st)
+    batched_pilots = [o[0].clone() for o in outs[:: max(1, len(outs) // 64)]]
+    # plain sequential builds of the same sets
+    for k in sets[:8]:
+        ctx.build(k, cfg, out=outs[0] if len(k) == len(sets[0]) else None)
+    lat = []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a.record(stream)
+    for k, o in zip(sets, outs):
+        t1 = time.perf_counter()
+        ctx.build(k, cfg, out=o)
+        lat.append(1e3 * (time.perf_counter() - t1))
+    b.record(stream)
+    torch.cuda.synchronize()
+    seq_wall = time.perf_counter() - t0
+    seq_dev = a.elapsed_time(b)
+    same = all(bool(torch.equal(p, o[0])) for p, o in zip(batched_pilots, outs[:: max(1, len(outs) // 64)]))
+    bad = sum(ctx.verify(sets[i], cfg, phobic.BuildResult(outs[i][0], outs[i][1], cfg.partitions(len(sets[i])), B))
+              for i in range(0, len(sets), max(1, len(sets) // 32)))
+    print(json.dumps({
+        "workload": "C4 batched build", "sets": len(sizes), "total_keys": total,
+        "config": {"lambda": lam, "partition_size": P, "sizes": "log-uniform [1e3, 4*2^20], seed 4", "data": "synthetic"},
+        "batched": {"wall_ms": 1e3 * batch_wall, "device_ms": batch_dev, "mkeys_per_s": total / batch_wall / 1e6,
+                    "kernel_launches": res[0].timings["kernels"]},
+        "sequential_plain": {"wall_ms": 1e3 * seq_wall, "device_ms": seq_dev, "mkeys_per_s": total / seq_wall / 1e6,
+                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                             "kernel_launches": 4 * len(sets)},
+        "speedup_batched_vs_sequential": seq_wall / batch_wall,
+        "batched_equals_plain_sample": same, "bijection_bad_sample": bad,
+    }), flush=True)
+    ctx.close()
+
+
+def run_c5(args) -> None:
+    """Served stream: Poisson arrivals at 200 req/s, sizes log-uniform in [1e4, 5e7], 70 % u64 /
+    30 % strings (seed 5), lambda 7, P 2048, device budget 120 GB; continuous batching on
+    several streams vs plain one-at-a-time builds (one stream, no batching) of the same stream."""
+    import torch
+
+    import keygen
+    import phobic
+
+    lam, P = 7.0, 2048
+    cfg = phobic.MPHFconfig(lam, P)
+    times, sizes, kinds = keygen.request_stream(5, 200.0, args.c5_seconds, 1e4, args.c5_max, 0.3)
+    rng = np.random.default_rng(55)
+    u64_pool = keygen.splitmix64_cuda(5, int(sizes.max()))
+    n_str = int(sizes[kinds == "strings"].max()) if (kinds == "strings").any() else 1
+    sd, so = keygen.strings(5, n_str)
+    sdata = torch.from_numpy(sd).cuda()
+    soffs = torch.from_numpy(so.view(np.int64)).cuda()
+    reqs = []
+    for t, n, k in zip(times, sizes, kinds):
+        n = int(n)
+        if k == "u64":
+            a = int(rng.integers(0, len(u64_pool) - n + 1))
+            reqs.append((t, phobic.KeySet(phobic.KEYS_U64, n, u64_pool[a:a + n], None, True)))
+        else:
+            a = int(rng.integers(0, n_str - n + 1))
+            reqs.append((t, phobic.KeySet(phobic.KEYS_STRINGS, n, sdata, soffs[a:a + n + 1], True)))
+    total = int(sizes.sum())
+
+    def replay(streams, max_batch):
+        outs = []
+        with phobic.Server(0, streams=streams, budget_bytes=120 << 30, max_batch_sets=max_batch) as srv:
+            t0 = time.perf_counter()
+            tickets = []
+            for t, ks in reqs:
+                delay = t - (time.perf_counter() - t0)
+                if delay > 0:
+                    time.sleep(delay)
+                tickets.append(srv.submit(ks, cfg))
+            for tk in tickets:
+                st, r = srv.wait(tk)
+                assert st == 0
+                outs.append(hashlib.sha1(np.ascontiguousarray(r.pilots).tobytes()).hexdigest())
+            wall = time.perf_counter() - t0
+            stats = srv.stats()
+        return outs, wall, stats
+
+    served, s_wall, s_stats = replay(4, 0)
+    plain, p_wall, p_stats = replay(1, 1)
+    same = served == plain
+    def summary(wall, st):
+        return {"wall_s": wall, "busy_s": st["busy_ms"] / 1e3, "mkeys_per_s_busy": total / (st["busy_ms"] / 1e3) / 1e6,
+                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                "peak_device_bytes": st["peak_bytes"]}
+    print(json.dumps({
+        "workload": "C5 served build stream", "requests": len(reqs), "total_keys": total,
+        "string_requests": int((kinds == "strings").sum()),
+        "config": {"rate_per_s": 200, "seconds": args.c5_seconds, "sizes": f"log-uniform [1e4, {args.c5_max:.0e}]",
+                   "lambda": lam, "partition_size": P, "budget_gb": 120, "results": "host memory",
+                   "keys": "device-resident pools, each request a slice", "data": "synthetic, seed 5"},
+        "served_continuous_batching": summary(s_wall, s_stats),
+        "plain_one_at_a_time": summary(p_wall, p_stats),
+        "results_identical": same,
+    }), flush=True)
 
 
 def main() -> None:
@@ -294,11 +503,30 @@ def main() -> None:
     ap.add_argument("--cpu-sample", type=int, default=20_000_000)
     ap.add_argument("--ref-sample", type=int, default=20_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2")
+    ap.add_argument("--c4-sets", type=int, default=4096)
+    ap.add_argument("--c5-seconds", type=float, default=60.0)
+    ap.add_argument("--c5-max", type=float, default=5e7)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
-    else:
+    elif args.workload == "c2":
         run_ours(args)
+    elif args.workload == "c1":
+        import keygen
+        import phobic
+        run_plain_workload(args, "C1", 5.0, 2048, lambda: (keygen.splitmix64(1, 1_000_000), phobic.KEYS_U64),
+                           "1M u64 splitmix64(seed=1), lambda 5, P 2048")
+    elif args.workload == "c3":
+        import keygen
+        import phobic
+        run_plain_workload(args, "C3", 6.0, 2048, lambda: (keygen.strings(3, args.n if args.n != 100_000_000 else 50_000_000),
+                                                           phobic.KEYS_STRINGS),
+                           "50M strings, length U[8,64], printable ASCII, seed 3, lambda 6, P 2048")
+    elif args.workload == "c4":
+        run_c4(args)
+    else:
+        run_c5(args)
 
 
 if __name__ == "__main__":

@@ -151,6 +151,21 @@ PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *
                                  const phobic_params *params, const phobic_result *results,
                                  phobic_status *statuses, phobic_timings *timings);
 
+/* ------------------------------------------------------------------ encoding
+ * Mphf::setData (mphf.hpp:65-75) on the host: encodes a build's pilots and
+ * partition offsets with the reference's encoders (same bytes as the reference)
+ * and serialises them in visit() order: the pilot encoder, then the partition-
+ * offset encoder; vectors as a size_t count followed by their elements.
+ * pilot_encoder: 0 interleaved<compact>, 1 interleaved<dictionary>, 2 interleaved<rice>,
+ * 3 mono<compact>, 4 mono<dictionary>, 5 interleaved_dual<rice,compact> (tradeoff),
+ * 6 interleaved<elias_fano>, 7 interleaved<sdc>, 8 mono<rice>.
+ * offset_encoder: 0 diff_partition<compact>, 1 direct_partition<compact>.
+ * Writes at most cap bytes to out (out may be NULL); *size = the full byte count. */
+PHOBIC_API phobic_status phobic_encode(int pilot_encoder, int offset_encoder, const uint32_t *pilots,
+                                       const uint32_t *partition_offsets, uint32_t partitions,
+                                       const phobic_params *params, float tradeoff, uint8_t *out, size_t cap,
+                                       size_t *size, double *bits_per_key);
+
 /* ------------------------------------------------------------------ query
  * MPHF::operator() (mphf.hpp:77-86) over the raw (unencoded) result arrays.
  * positions[i] = slot of key i in [0, n_built).  Arrays may live on the host
@@ -200,6 +215,7 @@ typedef struct phobic_server_config {
     int32_t device;
     uint32_t streams;        /* concurrent builds in flight (>= 1) */
     uint32_t queue_capacity; /* pending requests before submit returns PHOBIC_ERR_BUSY */
+    uint32_t max_batch_sets; /* requests built together in one batch; 0 = no limit, 1 = one at a time */
     uint64_t budget_bytes;   /* device memory the admitted builds may hold together */
 } phobic_server_config;
 

@@ -22,7 +22,7 @@ LIB = PKG / "lib" / "libphobic_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
-    "-Xcompiler", "-fPIC,-O3,-ffp-contract=off,-fvisibility=hidden",
+    "-Xcompiler", "-fPIC,-O3,-ffp-contract=off,-fvisibility=hidden,-fopenmp",
     "-Xptxas", "-O3",
     f"-I{ROOT / 'include'}", f"-I{CSRC}", f"-I{PKG / 'cpp'}",
 ]
@@ -65,7 +65,7 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
                 print("compiled", obj.name)
     objs = [OBJ / (s.stem + ".o") for s in sources]
     if todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread", "-lgomp"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stderr}")

@@ -165,6 +165,7 @@ void dispatch_loop(phobic_server *s) {
         const Request head = s->pending.front();
         for (auto it = s->pending.begin(); it != s->pending.end();) {
             if (!batch.empty() && (!same_group(*it, head) || nkeys + it->keys.n > kBatchKeyLimit ||
+                                   (s->cfg.max_batch_sets && batch.size() >= s->cfg.max_batch_sets) ||
                                    bytes + it->bytes > s->cfg.budget_bytes / (uint64_t)s->workers.size() + head.bytes)) {
                 ++it;
                 continue;

@@ -71,3 +71,21 @@ def request_stream(seed: int, rate: float, seconds: float, lo: int, hi: int, str
     sizes = np.floor(np.exp(rng.uniform(np.log(lo), np.log(hi), k))).astype(np.int64)
     kinds = np.where(rng.uniform(size=k) < string_frac, "strings", "u64")
     return np.array(times), sizes, kinds
+
+
+def splitmix64_cuda(seed: int, n: int, start: int = 0, device: str = "cuda"):
+    """The splitmix64 stream generated on the device (torch int64 with wrapping
+    arithmetic; logical shifts emulated by masking the arithmetic ones)."""
+    import torch
+
+    def s64(v: int) -> int:
+        return v - (1 << 64) if v >= 1 << 63 else v
+
+    def lsr(x, s: int):
+        return (x >> s) & ((1 << (64 - s)) - 1)
+
+    z = torch.arange(start + 1, start + n + 1, dtype=torch.int64, device=device)
+    z.mul_(s64(int(GAMMA))).add_(s64(seed % (1 << 64)))
+    z = (z ^ lsr(z, 30)).mul_(s64(int(M1)))
+    z = (z ^ lsr(z, 27)).mul_(s64(int(M2)))
+    return z ^ lsr(z, 31)

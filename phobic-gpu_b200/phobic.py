@@ -77,6 +77,7 @@ class ServerConfig(C.Structure):
         ("device", C.c_int32),
         ("streams", C.c_uint32),
         ("queue_capacity", C.c_uint32),
+        ("max_batch_sets", C.c_uint32),
         ("budget_bytes", C.c_uint64),
     ]
 
@@ -133,6 +134,9 @@ def _lib() -> C.CDLL:
         "phobic_query": (I32, [P, C.POINTER(Keys), C.POINTER(Params), U32, C.POINTER(Result), P]),
         "phobic_verify": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_debug_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P, P]),
+        "phobic_encode": (I32, [I32, I32, P, P, U32, C.POINTER(Params), C.c_float, P, C.c_size_t,
+                                C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
+        "phobic_build_noalloc": (I32, [C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P]),
         "phobic_server_create": (I32, [C.POINTER(ServerConfig), PP]),
         "phobic_server_submit": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_server_poll": (I32, [P, U64, C.POINTER(I32), C.POINTER(I32)]),
@@ -356,15 +360,38 @@ class MPHFbuilder:
         return self.ctx.build(keys, self.config, out)
 
 
+# ------------------------------------------------------------------ encoding
+
+PILOT_ENCODERS = {"interleaved_compact": 0, "interleaved_dictionary": 1, "interleaved_rice": 2, "mono_compact": 3,
+                  "mono_dictionary": 4, "dual_rice_compact": 5, "interleaved_elias_fano": 6, "interleaved_sdc": 7,
+                  "mono_rice": 8}
+OFFSET_ENCODERS = {"diff": 0, "direct": 1}
+
+
+def encode(built: BuildResult, cfg: MPHFconfig, pilot_encoder: str = "interleaved_compact",
+           offset_encoder: str = "diff", tradeoff: float = 0.5) -> tuple[bytes, float]:
+    """Mphf::setData on the host (the reference's encoders, same bytes): (serialised bytes, bits per key)."""
+    pil = np.ascontiguousarray(built.pilots, np.uint32)
+    off = np.ascontiguousarray(built.partition_offsets, np.uint32)
+    size, bpk = C.c_size_t(), C.c_double()
+    args = (PILOT_ENCODERS[pilot_encoder], OFFSET_ENCODERS[offset_encoder], pil.ctypes.data, off.ctypes.data,
+            built.partitions, C.byref(cfg.params), tradeoff)
+    check(_lib().phobic_encode(*args, None, 0, C.byref(size), C.byref(bpk)))
+    buf = np.zeros(size.value, np.uint8)
+    check(_lib().phobic_encode(*args, buf.ctypes.data, size.value, C.byref(size), C.byref(bpk)))
+    return buf.tobytes(), bpk.value
+
+
 # ------------------------------------------------------------------ batch and serving
 
-def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None = None):
-    """Build many key sets in one pass of the kernels; returns (results, statuses)."""
+def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None = None, outs_in: list | None = None):
+    """Build many key sets in one pass of the kernels; returns (results, statuses).
+    outs_in: optional (pilots, offsets) per set (e.g. CUDA tensors for device results)."""
     kss = [keyset(k, kind) for k in key_sets]
     arr = (Keys * len(kss))(*[k.struct() for k in kss])
     outs, res_structs = [], []
-    for ks in kss:
-        r, pil, off, parts = ctx._result(cfg, ks.n)
+    for i, ks in enumerate(kss):
+        r, pil, off, parts = ctx._result(cfg, ks.n, outs_in[i] if outs_in else None)
         outs.append(BuildResult(pil, off, parts, cfg.bucketCountPerPartition))
         res_structs.append(r)
     rarr = (Result * len(kss))(*res_structs)
@@ -381,24 +408,29 @@ def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None 
 class Server:
     """phobic_server: continuous-batching build server on one device."""
 
-    def __init__(self, device: int = 0, streams: int = 2, budget_bytes: int = 8 << 30, queue_capacity: int = 65536):
-        cfg = ServerConfig(device, streams, queue_capacity, budget_bytes)
+    def __init__(self, device: int = 0, streams: int = 2, budget_bytes: int = 8 << 30, queue_capacity: int = 65536,
+                 max_batch_sets: int = 0):
+        cfg = ServerConfig(device, streams, queue_capacity, max_batch_sets, budget_bytes)
         h = C.c_void_p()
         check(_lib().phobic_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h.value
         self._live = {}
 
-    def submit(self, keys, cfg: MPHFconfig, kind: int | None = None) -> int:
+    def submit(self, keys, cfg: MPHFconfig, kind: int | None = None, out=None) -> int:
+        """Queue one build; out = (pilots, offsets) arrays (host numpy or CUDA tensors) or None."""
         ks = keyset(keys, kind)
         parts = cfg.partitions(ks.n)
-        pil = np.zeros(max(cfg.bucketCountPerPartition * parts, 1), np.uint32)
-        off = np.zeros(parts + 1, np.uint32)
-        res = Result(0, pil.ctypes.data, off.ctypes.data)
+        if out is None:
+            pil = np.zeros(max(cfg.bucketCountPerPartition * parts, 1), np.uint32)
+            off = np.zeros(parts + 1, np.uint32)
+        else:
+            pil, off = out
+        res = Result(int(_is_cuda(pil)), _ptr(pil), _ptr(off))
         k = ks.struct()
         t = C.c_uint64()
         check(_lib().phobic_server_submit(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(t)))
-        self._live[t.value] = (ks, k, res, BuildResult(pil[: cfg.bucketCountPerPartition * parts], off, parts,
-                                                        cfg.bucketCountPerPartition))
+        self._live[t.value] = (ks, k, res, BuildResult(pil[: cfg.bucketCountPerPartition * parts] if out is None else pil,
+                                                        off, parts, cfg.bucketCountPerPartition))
         return int(t.value)
 
     def wait(self, ticket: int, timeout_ms: int = 600_000) -> tuple[int, BuildResult]:

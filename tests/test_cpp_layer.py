@@ -100,3 +100,16 @@ def test_reference_style_program_on_the_gpu(phobic, golden, tmp_path):
     assert "OK" in out.stdout
     want = golden["builds"]["C1_u64_seed1_n1e6_l5_P2048"]["encoded"]["interleaved_compact+diff"]
     assert hashlib.sha256(dump.read_bytes()).hexdigest() == want["sha256"]
+
+
+def test_abi_encode_matches_reference_golden(phobic, golden):
+    """phobic_encode (C ABI, host only) yields the reference encoders' bytes."""
+    B, f = O.config(7.0, 2500)
+    r = O.build(O.hash_keys(O.splitmix64(2, 2_000_000), "u64"), 2500, B, f)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    built = phobic.BuildResult(r["pilots"], r["offsets"], r["partitions"], B)
+    want = golden["builds"]["C2_sample_u64_seed2_n2e6_l7_P2500"]["encoded"]
+    for name in NAMES.values():
+        for off_name in ("diff", "direct"):
+            data, bpk = phobic.encode(built, cfg, name, off_name)
+            assert hashlib.sha256(data).hexdigest() == want[f"{name}+{off_name}"]["sha256"], (name, off_name)
