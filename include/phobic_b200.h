@@ -151,6 +151,12 @@ PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *
                                  const phobic_params *params, const phobic_result *results,
                                  phobic_status *statuses, phobic_timings *timings);
 
+/* Failure-detection hook: runs the partition-offset scan with its first tile never
+ * scheduled, so the next tile's look-back waits on a flag that nothing sets.  The
+ * kernel's bounded wait (wait_ms) must give up and record PHOBIC_ERR_TIMEOUT, which is
+ * returned in *observed; the context stays usable afterwards. */
+PHOBIC_API phobic_status phobic_debug_stalled_wait(phobic_ctx *ctx, uint32_t wait_ms, phobic_status *observed);
+
 /* ------------------------------------------------------------------ encoding
  * Mphf::setData (mphf.hpp:65-75) on the host: encodes a build's pilots and
  * partition offsets with the reference's encoders (same bytes as the reference)

@@ -212,6 +212,12 @@ phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *keys, const
     return finish_sets(ctx->w, nullptr, nullptr, &ctx->last_error);
 }
 
+phobic_status phobic_debug_stalled_wait(phobic_ctx *ctx, uint32_t wait_ms, phobic_status *observed) {
+    if (!ctx || !observed) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return run_stalled_wait(ctx->w, wait_ms, observed, &ctx->last_error);
+}
+
 phobic_status phobic_query(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params, uint32_t partitions,
                            const phobic_result *built, uint32_t *positions) {
     if (!ctx) return PHOBIC_ERR_INVALID;

@@ -14,7 +14,14 @@ constexpr uint32_t kMaxBucket = 256;         // sort_sum.comp bins cover sizes 1
 constexpr uint32_t kDupCheckAt = 256;        // pilot counter at which a bucket is checked for duplicate keys
 constexpr uint32_t kDefaultMaxPilot = 1u << 20;
 constexpr unsigned long long kNoError = ~0ull;
-constexpr uint32_t kSpinLimit = 1u << 26;    // bound of every spin-wait in the kernels
+constexpr unsigned long long kSpinTimeoutNs = 1000000000ull;  // default bound of every spin-wait: 1 s
+
+// Nanosecond clock shared by all SMs, for time-bounded waits.
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 
 // Error word: the smallest (partition << 32 | code) wins, so the reported error is
 // the one of the lowest partition, and errors found before the search (code INVALID

@@ -213,7 +213,8 @@ uint64_t sets_arena_bytes(const phobic_keys *sets, uint32_t nsets, const phobic_
     }
     t += align256(4 * kFulcrums) + align256(sizeof(SetDesc) * nsets) + 2 * align256(8 * (nsets + 1)) +
          align256(8 * nsets) + align256(64);
-    t += align256(4 * M) + align256(4 * (M + 1)) + align256(8 * ((M + kScanTile - 1) / kScanTile) + 8);
+    const uint64_t MS = M * kSub;
+    t += align256(4 * MS) + align256(4 * (MS + 1)) + align256(8 * ((MS + kScanTile - 1) / kScanTile) + 8);
     if (nsets && sets[0].kind == PHOBIC_KEYS_STRINGS) t += align256(16 * N);
     t += align256(8 * N) + align256(2 * N) + align256(8 * N);  // lowers, bucket ids, sorted
     if (debug) t += align256(16 * N) + align256(4 * M * B);
@@ -253,7 +254,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         N += sets[s].n;
         M += (sets[s].n + P - 1) / P;
     }
-    if (N > 0xFFFFFFFFull || M > 0xFFFFFFFFull) {
+    if (N > 0xFFFFFFFFull || M * kSub > 0xFFFFFFFFull) {
         if (err) *err = "a build holds at most 2^32-1 keys in total";
         return PHOBIC_ERR_INVALID;
     }
@@ -327,9 +328,10 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     uint32_t *d_pb = static_cast<uint32_t *>(take(8 * (nsets + 1)));
     unsigned long long *d_err = static_cast<unsigned long long *>(take(8 * nsets));
     uint32_t *d_queue = static_cast<uint32_t *>(take(64));
-    uint32_t *d_count = static_cast<uint32_t *>(take(4 * M));
-    uint32_t *d_G = static_cast<uint32_t *>(take(4 * (M + 1)));
-    const uint32_t tiles = (uint32_t)((M + kScanTile - 1) / kScanTile);
+    const uint64_t MS = M * kSub;  // sub-counters
+    uint32_t *d_count = static_cast<uint32_t *>(take(4 * MS));
+    uint32_t *d_G = static_cast<uint32_t *>(take(4 * (MS + 1)));
+    const uint32_t tiles = (uint32_t)((MS + kScanTile - 1) / kScanTile);
     unsigned long long *d_tiles = static_cast<unsigned long long *>(take(8 * (size_t)tiles + 8));
     uint4 *d_mapped = kind == PHOBIC_KEYS_STRINGS ? static_cast<uint4 *>(take(16 * N)) : nullptr;
     uint2 *d_lowers = static_cast<uint2 *>(take(8 * N));
@@ -347,7 +349,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     PHB_TRY(cudaMemcpyAsync(d_pb, hpb, 4 * (nsets + 1), cudaMemcpyHostToDevice, s), "H2D sets");
     PHB_TRY(cudaMemsetAsync(d_err, 0xFF, 8 * nsets, s), "memset");
     PHB_TRY(cudaMemsetAsync(d_queue, 0, 64, s), "memset");
-    PHB_TRY(cudaMemsetAsync(d_count, 0, 4 * M, s), "memset");
+    PHB_TRY(cudaMemsetAsync(d_count, 0, 4 * MS, s), "memset");
     PHB_TRY(cudaMemsetAsync(d_tiles, 0, 8 * (size_t)tiles + 8, s), "memset");
     if (M == 0) PHB_TRY(cudaMemsetAsync(d_G, 0, 4, s), "memset");
     PHB_TRY(cudaEventRecord(w.ev[1], s), "event");
@@ -356,8 +358,8 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     MapArgs ma{d_desc, d_kb, nsets, B, N, d_fulcs, d_count, d_mapped, d_dbg_keys, d_lowers, d_bkt, d_err};
     PHB_TRY(launch_map_count(kind, ma, grid, s), "K1 map_count");
     PHB_TRY(cudaEventRecord(w.ev[2], s), "event");
-    ScanArgs sa{d_count, d_G, d_count, (uint32_t)M, cap, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles),
-                d_pb, nsets, d_err};
+    ScanArgs sa{d_count, d_G, d_count, (uint32_t)MS, cap, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles),
+                d_pb, nsets, d_err, 0};
     PHB_TRY(launch_scan(sa, s), "K2 scan");
     PHB_TRY(cudaEventRecord(w.ev[3], s), "event");
     PHB_TRY(launch_scatter(kind, ma, grid, s), "K3 scatter");
@@ -433,6 +435,38 @@ phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t,
         }
     }
     return first;
+}
+
+// ------------------------------------------------------------------ bounded-wait test
+
+phobic_status run_stalled_wait(Worker &w, uint32_t wait_ms, phobic_status *observed, std::string *err) {
+    PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
+    const uint32_t m = 2 * kScanTile;  // two tiles: tile 1 waits on tile 0, which never runs
+    w.arena.reset();
+    PHB_TRY(w.arena.reserve(align256(4 * m) + align256(4 * (m + 1)) + align256(8 * 2 + 8) + align256(8) + 4096),
+            "device arena");
+    uint32_t *d_in = static_cast<uint32_t *>(w.arena.take(4 * m));
+    uint32_t *d_out = static_cast<uint32_t *>(w.arena.take(4 * (m + 1)));
+    unsigned long long *d_tiles = static_cast<unsigned long long *>(w.arena.take(8 * 2 + 8));
+    unsigned long long *d_err = static_cast<unsigned long long *>(w.arena.take(8));
+    uint32_t one_base[2] = {0, m / kSub};
+    uint32_t *d_pb = static_cast<uint32_t *>(w.arena.take(8));
+    cudaStream_t s = w.stream;
+    PHB_TRY(cudaMemsetAsync(d_in, 0, 4 * m, s), "memset");
+    PHB_TRY(cudaMemsetAsync(d_tiles, 0, 8 * 2 + 8, s), "memset");
+    PHB_TRY(cudaMemsetAsync(d_err, 0xFF, 8, s), "memset");
+    PHB_TRY(cudaMemcpyAsync(d_pb, one_base, sizeof(one_base), cudaMemcpyHostToDevice, s), "H2D");
+    ScanArgs sa{d_in, d_out, nullptr, m, 0xFFFFFFFFu, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + 2), d_pb, 1,
+                d_err, (unsigned long long)wait_ms * 1000000ull};
+    PHB_TRY(launch_scan_stalled(sa, 1, s), "stalled scan");
+    PHB_TRY(w.pinned.reserve(4096), "pinned");
+    unsigned long long *h = static_cast<unsigned long long *>(w.pinned.data());
+    PHB_TRY(cudaMemcpyAsync(h, d_err, 8, cudaMemcpyDeviceToHost, s), "D2H");
+    PHB_TRY(cudaEventRecord(w.ev[7], s), "event");
+    phobic_status st = wait_event(w.ev[7], w.timeout_ms, err);
+    if (st != PHOBIC_OK) return st;
+    *observed = *h == kNoError ? PHOBIC_OK : (phobic_status)(uint32_t)*h;
+    return PHOBIC_OK;
 }
 
 // ------------------------------------------------------------------ query

@@ -91,6 +91,10 @@ phobic_status cuda_status(cudaError_t e, const char *what, std::string *err);
 phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params *params, uint32_t partitions,
                         const phobic_result *built, uint32_t *positions, uint64_t *bad, std::string *err);
 
+// Runs the scan with a never-scheduled first tile (bounded-wait test); *observed gets
+// the status the kernel recorded.
+phobic_status run_stalled_wait(Worker &w, uint32_t wait_ms, phobic_status *observed, std::string *err);
+
 // Default search bitmap capacity for a partition size (search.comp:21).
 uint32_t default_max_partition(uint32_t partition_size);
 

@@ -17,6 +17,10 @@
 namespace phobicb200 {
 
 constexpr int kMapThreads = 256;
+// Each partition's keys are counted and scattered through kSub sub-counters
+// (key index mod kSub), whose slot ranges are adjacent: a partition stays
+// contiguous, and the atomics of one partition spread over kSub addresses.
+constexpr uint32_t kSub = 8;
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;  // partitions per thread: one tile = 4096 partitions
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -55,7 +59,7 @@ struct MapArgs {
     uint32_t buckets;
     uint64_t total_keys;
     const uint32_t *fulcs;     // [2048]
-    uint32_t *counts;          // K1: [M] zeroed;   K3: cursors (start = record offset)
+    uint32_t *counts;          // [M * kSub] K1: zeroed counts;  K3: cursors (start = record offset)
     uint4 *mapped;             // strings: [total] {global partition, bucket, lower1, lower2}
     uint4 *debug_keys;         // [total] hashed Keys (debug builds) or null
     uint2 *lowers;             // K3 output [total]
@@ -64,16 +68,17 @@ struct MapArgs {
 };
 
 struct ScanArgs {
-    const uint32_t *in;              // [m] partition sizes
+    const uint32_t *in;              // [m] sub-counter sizes, kSub per partition
     uint32_t *out;                   // [m + 1] exclusive prefix, out[m] = total
     uint32_t *cursor;                // [m] copy of out[0..m) (scatter cursors) or null
-    uint32_t m;
-    uint32_t cap;                    // largest allowed partition
+    uint32_t m;                      // partitions * kSub
+    uint32_t cap;                    // largest allowed partition (sum of its kSub counters)
     unsigned long long *tile_state;  // [tiles], zeroed: (flag << 32) | value
     uint32_t *tile_counter;          // zeroed
     const uint32_t *part_base;       // [nsets + 1] to name the set of an overflowing partition
     uint32_t nsets;
     unsigned long long *err;         // [nsets]
+    unsigned long long wait_ns;      // bound of the look-back wait on a predecessor tile
 };
 
 struct SearchArgs {
@@ -81,7 +86,7 @@ struct SearchArgs {
     const uint32_t *part_base;  // [nsets + 1]
     uint32_t nsets;
     uint32_t M;                 // global partitions
-    const uint32_t *G;          // [M + 1] record offsets
+    const uint32_t *G;          // [M * kSub + 1] record offsets; partition g spans [G[g*kSub], G[(g+1)*kSub])
     const uint2 *lowers;        // partition-contiguous records
     const uint16_t *bkt;
     uint2 *sorted;              // scratch, same indexing as lowers
@@ -132,6 +137,10 @@ int search_warps_per_cta(uint32_t buckets, uint32_t cap);
 cudaError_t launch_map_count(int kind, const MapArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_scatter(int kind, const MapArgs &a, int grid, cudaStream_t st);
 cudaError_t launch_scan(const ScanArgs &a, cudaStream_t st);
+// The scan with its first `skip` tile ids never handed out, so the tiles after them
+// wait on predecessors that never publish: the bounded wait must end in
+// PHOBIC_ERR_TIMEOUT (failure-detection tests).
+cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t st);
 cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st);
 cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,
                          cudaStream_t st);

@@ -7,10 +7,11 @@
 //
 // K3 replaces apply_partition_offset.comp:9-18 and redistribute_keys.comp:21-53:
 // each key's (lower1, lower2) pair and bucket id are appended to its partition
-// through a per-partition cursor that K2 set to the partition's first record.
-// Appending in arrival order keeps each partition's write front inside one or
-// two L2 sectors, so the scattered 8-byte and 2-byte stores merge in L2 before
-// they reach HBM.  The bucket order inside a partition is produced later, in
+// through one of the partition's kSub cursors (chosen by the key index) that K2
+// set to the start of that cursor's slot range.  Appending in arrival order keeps
+// every write front inside one or two L2 sectors, so the scattered 8-byte and
+// 2-byte stores merge in L2 before they reach HBM; spreading a partition over
+// kSub cursors keeps same-address atomics from queueing behind each other.  The bucket order inside a partition is produced later, in
 // shared memory, by K4.
 #include "kernels.cuh"
 
@@ -81,7 +82,8 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
             uint32_t slot[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; u++)
-                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&a.counts[gp[u]], 1u);
+                if (gp[u] != 0xFFFFFFFFu)
+                    slot[u] = atomicAdd(&a.counts[(size_t)gp[u] * kSub + ((g0 + u * stride) & (kSub - 1))], 1u);
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
-                atomicAdd(&a.counts[gp[u]], 1u);
+                atomicAdd(&a.counts[(size_t)gp[u] * kSub + ((g0 + u * stride) & (kSub - 1))], 1u);
                 if (KIND == PHOBIC_KEYS_STRINGS) a.mapped[g0 + u * stride] = make_uint4(gp[u], b[u], l1[u], l2[u]);
             }
         }

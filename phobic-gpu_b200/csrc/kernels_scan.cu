@@ -9,7 +9,8 @@
 // reference leaves unchecked (search.comp:21).
 //
 // Each CTA takes the next tile id from a counter, so every tile it waits on was
-// started before it; the wait on a predecessor is still bounded (kSpinLimit).
+// started before it; the wait on a predecessor is still bounded in time
+// (ScanArgs::wait_ns), after which the CTA reports PHOBIC_ERR_TIMEOUT and ends.
 #include "kernels.cuh"
 
 namespace phobicb200 {
@@ -36,20 +37,22 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
     if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
+    if ((uint64_t)tile * kScanTile >= a.m) return;  // only when tile ids were skipped on purpose
     const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
 
+    static_assert(kScanItems == kSub, "one thread holds the kSub counters of one partition");
     uint32_t v[kScanItems];
-    uint32_t sum = 0, over_at = 0xFFFFFFFFu;
+    uint32_t sum = 0;
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {
         uint64_t idx = base + j;
         v[j] = idx < a.m ? a.in[idx] : 0u;
-        if (v[j] > a.cap && over_at == 0xFFFFFFFFu) over_at = (uint32_t)idx;
         sum += v[j];
     }
-    if (over_at != 0xFFFFFFFFu) {
-        uint32_t set = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, over_at);
-        report_error(&a.err[set], over_at - a.part_base[set], PHOBIC_ERR_PARTITION_OVERFLOW);
+    if (sum > a.cap) {  // this thread's items are the sub-counters of partition base / kSub
+        const uint32_t part = (uint32_t)(base / kSub);
+        uint32_t set = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, part);
+        report_error(&a.err[set], part - a.part_base[set], PHOBIC_ERR_PARTITION_OVERFLOW);
     }
 
     uint32_t incl = warp_incl_scan(sum, lane);
@@ -71,15 +74,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
         } else {
             atomicExch(&a.tile_state[tile], kFlagAggregate | total);
             int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
+            const unsigned long long t0 = global_ns();
             while (j >= 0) {
                 unsigned long long s = *reinterpret_cast<volatile unsigned long long *>(&a.tile_state[j]);
                 unsigned long long flag = s & ~0xFFFFFFFFull;
                 if (flag == 0) {
-                    if (++spins > kSpinLimit) {
+                    if (global_ns() - t0 > a.wait_ns) {
                         for (uint32_t q = 0; q < a.nsets; q++) report_error(&a.err[q], 0, PHOBIC_ERR_TIMEOUT);
                         break;
                     }
+                    __nanosleep(200);
                     continue;
                 }
                 prefix += (uint32_t)s;
@@ -109,7 +113,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
 cudaError_t launch_scan(const ScanArgs &a, cudaStream_t st) {
     if (a.m == 0) return cudaSuccess;
     uint32_t tiles = (a.m + kScanTile - 1) / kScanTile;
-    k_scan<<<tiles, kScanThreads, 0, st>>>(a);
+    ScanArgs b = a;
+    if (!b.wait_ns) b.wait_ns = kSpinTimeoutNs;
+    k_scan<<<tiles, kScanThreads, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+__global__ void k_skip_tiles(uint32_t *tile_counter, uint32_t skip) { *tile_counter = skip; }
+
+cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t st) {
+    if (a.m == 0) return cudaSuccess;
+    uint32_t tiles = (a.m + kScanTile - 1) / kScanTile;
+    k_skip_tiles<<<1, 1, 0, st>>>(a.tile_counter, skip);
+    ScanArgs b = a;
+    if (!b.wait_ns) b.wait_ns = kSpinTimeoutNs;
+    k_scan<<<tiles, kScanThreads, 0, st>>>(b);
     return cudaGetLastError();
 }
 

@@ -242,8 +242,8 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
 __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
                                                      uint32_t g, uint32_t p, int lane) {
     const uint32_t B = a.buckets;
-    const uint32_t base = a.G[g];
-    const uint32_t ps = a.G[g + 1] - base;
+    const uint32_t base = a.G[(size_t)g * kSub];
+    const uint32_t ps = a.G[(size_t)(g + 1) * kSub] - base;
     if (ps > a.cap) return PHOBIC_OK;  // reported by the scan
     const uint32_t ow = occ_words(a.cap);
     uint32_t *pil = d.pilots + p;
@@ -376,9 +376,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 4) k_search(SearchArgs a) {
         const SetDesc &d = a.sets[s];
         const uint32_t p = g - d.part_base;
         if (lane == 0 && d.part_off) {
-            const uint32_t g0 = a.G[d.part_base];
-            d.part_off[p] = a.G[g] - g0;
-            if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[g + 1] - g0;
+            const uint32_t g0 = a.G[(size_t)d.part_base * kSub];
+            d.part_off[p] = a.G[(size_t)g * kSub] - g0;
+            if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[(size_t)(g + 1) * kSub] - g0;
         }
         const uint32_t code = search_partition(a, ws, d, g, p, lane);
         if (code != PHOBIC_OK && lane == 0) report_error(&a.err[s], p, code);

@@ -134,6 +134,7 @@ def _lib() -> C.CDLL:
         "phobic_query": (I32, [P, C.POINTER(Keys), C.POINTER(Params), U32, C.POINTER(Result), P]),
         "phobic_verify": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_debug_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P, P]),
+        "phobic_debug_stalled_wait": (I32, [P, U32, C.POINTER(I32)]),
         "phobic_encode": (I32, [I32, I32, P, P, U32, C.POINTER(Params), C.c_float, P, C.c_size_t,
                                 C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
         "phobic_build_noalloc": (I32, [C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P]),
@@ -334,6 +335,12 @@ class Context:
         check(_lib().phobic_query(self.handle, C.byref(k), C.byref(cfg.params), built.partitions, C.byref(res),
                                   pos.ctypes.data), self)
         return pos[: ks.n]
+
+    def stalled_wait(self, wait_ms: int) -> int:
+        """Status recorded by a kernel whose bounded wait on a never-set flag ran out."""
+        st = C.c_int()
+        check(_lib().phobic_debug_stalled_wait(self.handle, wait_ms, C.byref(st)), self)
+        return int(st.value)
 
     def verify(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None) -> int:
         """Number of keys whose slot is out of range or taken twice (0 = bijection)."""

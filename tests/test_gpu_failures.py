@@ -1,0 +1,37 @@
+"""Failure detection on the GPU without faulting it: a kernel wait that nothing
+releases must give up after its bound and report a status the host reads, and the
+context must keep working afterwards."""
+import time
+
+import pytest
+
+import keygen
+
+pytestmark = pytest.mark.gpu
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(phobic):
+    with phobic.Context(0) as ctx:
+        t0 = time.perf_counter()
+        observed = ctx.stalled_wait(300)
+        elapsed = time.perf_counter() - t0
+        assert observed == phobic.ERR_TIMEOUT
+        assert 0.25 < elapsed < 30
+        cfg = phobic.MPHFconfig(7.0, 2500)
+        keys = keygen.splitmix64(3, 200_000)
+        got = ctx.build(keys, cfg)
+        assert ctx.verify(keys, cfg, got) == 0
+
+
+def test_errors_leave_other_sets_of_a_batch_intact(phobic):
+    """A failing set (duplicate keys) in a batch reports its own status; the other
+    sets' results are complete and correct."""
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    good = [keygen.splitmix64(60 + i, 20_000) for i in range(3)]
+    bad = keygen.splitmix64(70, 20_000)
+    bad[11] = bad[5]
+    with phobic.Context(0) as ctx:
+        outs, st = phobic.build_batch(ctx, [good[0], bad, good[1], good[2]], cfg)
+        assert st == [0, phobic.ERR_DUPLICATE_KEY, 0, 0]
+        for keys, res in zip(good, [outs[0], outs[2], outs[3]]):
+            assert ctx.verify(keys, cfg, res) == 0
