@@ -274,7 +274,7 @@ def run_ours(args) -> None:
                    "l2": "inputs larger than L2 (800 MB keys per step)"},
         "stages_ms": {k: round(v, 4) for k, v in stage.items() if k != "kernels"},
         "bijection_bad": bad, "host_result_equals_device": same,
-        "gpu_launches": 4 * args.steps,
+        "gpu_launches": int(stage["kernels"]) * args.steps,
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mkeys/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 4 * (parts * B + parts + 1), "ms_per_step": e2e_ms,
                 "device_ms_per_step": statistics.mean(e2e_dev)},

@@ -49,6 +49,8 @@ def _compile(src: Path, extra: list[str]) -> Path:
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src.name}:\n{res.stderr}")
+    if extra and res.stderr:
+        print(res.stderr, end="")
     return obj
 
 

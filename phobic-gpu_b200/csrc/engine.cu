@@ -213,10 +213,11 @@ uint64_t sets_arena_bytes(const phobic_keys *sets, uint32_t nsets, const phobic_
     }
     t += align256(4 * kFulcrums) + align256(sizeof(SetDesc) * nsets) + 2 * align256(8 * (nsets + 1)) +
          align256(8 * nsets) + align256(64);
-    const uint64_t MS = M * kSub;
+    const uint64_t MS = M * plan_map(N, M, 0).stride;  // count matrix entries
     t += align256(4 * MS) + align256(4 * (MS + 1)) + align256(8 * ((MS + kScanTile - 1) / kScanTile) + 8);
     if (nsets && sets[0].kind == PHOBIC_KEYS_STRINGS) t += align256(16 * N);
-    t += align256(8 * N) + align256(2 * N) + align256(8 * N);  // lowers, bucket ids, sorted
+    // lowers, bucket ids, partition records (also the search's scratch), cursors
+    t += align256(8 * N) + align256(2 * N) + align256(16 * N) + align256(4 * M) + align256(4 * kMaxBins);
     if (debug) t += align256(16 * N) + align256(4 * M * B);
     return t + 4096;
 }
@@ -254,7 +255,8 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         N += sets[s].n;
         M += (sets[s].n + P - 1) / P;
     }
-    if (N > 0xFFFFFFFFull || M * kSub > 0xFFFFFFFFull) {
+    const MapPlan plan = plan_map(N, M, w.sm_count);
+    if (N > 0xFFFFFFFFull || M * plan.stride > 0xFFFFFFFFull) {
         if (err) *err = "a build holds at most 2^32-1 keys in total";
         return PHOBIC_ERR_INVALID;
     }
@@ -328,7 +330,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     uint32_t *d_pb = static_cast<uint32_t *>(take(8 * (nsets + 1)));
     unsigned long long *d_err = static_cast<unsigned long long *>(take(8 * nsets));
     uint32_t *d_queue = static_cast<uint32_t *>(take(64));
-    const uint64_t MS = M * kSub;  // sub-counters
+    const uint64_t MS = M * plan.stride;  // count matrix entries
     uint32_t *d_count = static_cast<uint32_t *>(take(4 * MS));
     uint32_t *d_G = static_cast<uint32_t *>(take(4 * (MS + 1)));
     const uint32_t tiles = (uint32_t)((MS + kScanTile - 1) / kScanTile);
@@ -336,10 +338,13 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     uint4 *d_mapped = kind == PHOBIC_KEYS_STRINGS ? static_cast<uint4 *>(take(16 * N)) : nullptr;
     uint2 *d_lowers = static_cast<uint2 *>(take(8 * N));
     uint16_t *d_bkt = static_cast<uint16_t *>(take(2 * N));
-    uint2 *d_sorted = static_cast<uint2 *>(take(8 * N));
+    uint4 *d_inter = static_cast<uint4 *>(take(16 * N));
+    uint2 *d_sorted = reinterpret_cast<uint2 *>(d_inter);  // K4 scratch, after K3 is done with d_inter
+    uint32_t *d_pcur = static_cast<uint32_t *>(take(4 * M));
+    uint32_t *d_bincur = static_cast<uint32_t *>(take(4 * kMaxBins));
     uint4 *d_dbg_keys = debug ? static_cast<uint4 *>(take(16 * N)) : nullptr;
     uint32_t *d_dbg_sizes = debug ? static_cast<uint32_t *>(take(4 * M * B)) : nullptr;
-    if (!d_sorted || (debug && !d_dbg_sizes)) {
+    if (!d_bincur || (debug && !d_dbg_sizes)) {
         if (err) *err = "arena sizing error";
         return PHOBIC_ERR_OOM;
     }
@@ -354,18 +359,23 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     if (M == 0) PHB_TRY(cudaMemsetAsync(d_G, 0, 4, s), "memset");
     PHB_TRY(cudaEventRecord(w.ev[1], s), "event");
 
-    const int grid = (int)std::min<uint64_t>((N + kMapThreads - 1) / kMapThreads, (uint64_t)w.sm_count * 8);
-    MapArgs ma{d_desc, d_kb, nsets, B, N, d_fulcs, d_count, d_mapped, d_dbg_keys, d_lowers, d_bkt, d_err};
-    PHB_TRY(launch_map_count(kind, ma, grid, s), "K1 map_count");
+    MapArgs ma{d_desc, d_kb, nsets, B, N, d_fulcs, d_count, d_mapped, d_dbg_keys, d_lowers, d_bkt, d_err,
+               (uint32_t)M, plan.stride, plan.chunk};
+    // K1, scan, size check, two partition passes, search; none when there are no keys.
+    w.pending_kernels = N ? 6 : 0;
+    PHB_TRY(launch_map_count(kind, ma, plan, s), "K1 map_count");
     PHB_TRY(cudaEventRecord(w.ev[2], s), "event");
-    ScanArgs sa{d_count, d_G, d_count, (uint32_t)MS, cap, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles),
-                d_pb, nsets, d_err, 0};
+    ScanArgs sa{d_count, d_G, nullptr, (uint32_t)MS, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles), nsets,
+                d_err, 0};
     PHB_TRY(launch_scan(sa, s), "K2 scan");
+    const uint32_t wshift = part_wshift(M);
+    PartArgs pa{d_inter, d_bincur, d_pcur, wshift, (uint32_t)((M + (1ull << wshift) - 1) >> wshift)};
+    PHB_TRY(launch_check_sizes(d_G, (uint32_t)M, plan.stride, cap, d_pb, nsets, d_err, &pa, s), "K2 size check");
     PHB_TRY(cudaEventRecord(w.ev[3], s), "event");
-    PHB_TRY(launch_scatter(kind, ma, grid, s), "K3 scatter");
+    PHB_TRY(launch_partition(kind, ma, pa, w.sm_count, s), "K3 partition");
     PHB_TRY(cudaEventRecord(w.ev[4], s), "event");
-    SearchArgs qa{d_desc, d_pb, nsets, (uint32_t)M, d_G, d_lowers, d_bkt, d_sorted, d_dbg_sizes, B, cap, k_max,
-                  d_queue, d_err};
+    SearchArgs qa{d_desc, d_pb, nsets, (uint32_t)M, d_G, plan.stride, d_lowers, d_bkt, d_sorted, d_dbg_sizes, B, cap,
+                  k_max, d_queue, d_err};
     PHB_TRY(launch_search(qa, w.sm_count, s), "K4 search");
     PHB_TRY(cudaEventRecord(w.ev[5], s), "event");
 
@@ -420,7 +430,7 @@ phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t,
         t->search = elapsed(w.ev[4], w.ev[5]);
         t->result_transfer = elapsed(w.ev[5], w.ev[6]);
         t->total = elapsed(w.ev[0], w.ev[6]);
-        t->kernels = 4;
+        t->kernels = w.pending_kernels;
     }
     phobic_status first = PHOBIC_OK;
     for (uint32_t i = 0; i < w.pending_sets; i++) {
@@ -449,15 +459,13 @@ phobic_status run_stalled_wait(Worker &w, uint32_t wait_ms, phobic_status *obser
     uint32_t *d_out = static_cast<uint32_t *>(w.arena.take(4 * (m + 1)));
     unsigned long long *d_tiles = static_cast<unsigned long long *>(w.arena.take(8 * 2 + 8));
     unsigned long long *d_err = static_cast<unsigned long long *>(w.arena.take(8));
-    uint32_t one_base[2] = {0, m / kSub};
-    uint32_t *d_pb = static_cast<uint32_t *>(w.arena.take(8));
+
     cudaStream_t s = w.stream;
     PHB_TRY(cudaMemsetAsync(d_in, 0, 4 * m, s), "memset");
     PHB_TRY(cudaMemsetAsync(d_tiles, 0, 8 * 2 + 8, s), "memset");
     PHB_TRY(cudaMemsetAsync(d_err, 0xFF, 8, s), "memset");
-    PHB_TRY(cudaMemcpyAsync(d_pb, one_base, sizeof(one_base), cudaMemcpyHostToDevice, s), "H2D");
-    ScanArgs sa{d_in, d_out, nullptr, m, 0xFFFFFFFFu, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + 2), d_pb, 1,
-                d_err, (unsigned long long)wait_ms * 1000000ull};
+    ScanArgs sa{d_in, d_out, nullptr, m, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + 2), 1, d_err,
+                (unsigned long long)wait_ms * 1000000ull};
     PHB_TRY(launch_scan_stalled(sa, 1, s), "stalled scan");
     PHB_TRY(w.pinned.reserve(4096), "pinned");
     unsigned long long *h = static_cast<unsigned long long *>(w.pinned.data());

@@ -53,6 +53,7 @@ struct Worker {
     DeviceArena arena;
     PinnedBuffer pinned;  // set table on the way in, per-set error words on the way out
     uint32_t pending_sets = 0;
+    uint32_t pending_kernels = 0;  // kernels the last enqueued build launched
     unsigned long long *pending_err = nullptr;  // host view of the error words of the last build
     uint64_t timeout_ms = 120000;
 

@@ -1,7 +1,8 @@
 // Kernel argument blocks and launch entry points of the construction pipeline.
 //
-//   K1 map_count  keys -> per-partition key counts                 (kernels_map.cu)
-//   K2 scan       counts -> record offsets + scatter cursors        (kernels_scan.cu)
+//   K1 map_count  keys -> key counts per (partition, chunk)         (kernels_map.cu)
+//   K2 scan       counts -> record offsets (= scatter cursors)      (kernels_scan.cu)
+//                 + partition size check
 //   K3 scatter    keys -> partition-contiguous (lower pair, bucket) records
 //   K4 search     per partition: bucket sort + pilot search         (kernels_search.cu)
 //   Q  query      keys -> slots, bijection check                    (kernels_query.cu)
@@ -17,12 +18,16 @@
 namespace phobicb200 {
 
 constexpr int kMapThreads = 256;
-// Each partition's keys are counted and scattered through kSub sub-counters
-// (key index mod kSub), whose slot ranges are adjacent: a partition stays
-// contiguous, and the atomics of one partition spread over kSub addresses.
-constexpr uint32_t kSub = 8;
+// Chunked counting: CTA c owns the keys [c * chunk, (c + 1) * chunk) and keeps a
+// counter for every partition in shared memory; the count matrix is stored
+// partition-major (entry g * stride + c, stride = number of chunks), so its
+// exclusive scan gives each chunk its own slot range inside every partition.
+constexpr int kChunkThreads = 1024;
+constexpr uint32_t kChunkCtas = 148;                 // one CTA per SM of a B200
+constexpr uint64_t kChunkMinKeys = 16384;            // smallest chunk worth a CTA
+constexpr uint32_t kChunkMaxPartitions = 52 * 1024;  // shared-memory counters per CTA
 constexpr int kScanThreads = 512;
-constexpr int kScanItems = 8;  // partitions per thread: one tile = 4096 partitions
+constexpr int kScanItems = 8;  // entries per thread: one tile = 4096 entries
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kSearchWarps = 8;
 constexpr size_t kSearchSmemLimit = 227 * 1024;
@@ -52,6 +57,16 @@ __device__ __forceinline__ uint32_t find_set(const T *base, uint32_t nsets, T x)
     return lo;
 }
 
+// Launch plan of K1/K3: chunked shared-memory counters when every partition's
+// counter fits in one CTA's shared memory, else one global counter per partition.
+struct MapPlan {
+    bool chunked;
+    uint32_t stride;  // count-matrix entries per partition (chunks, or 1)
+    uint32_t grid;
+    uint64_t chunk;   // keys per CTA (chunked plan)
+};
+MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count);
+
 struct MapArgs {
     const SetDesc *sets;
     const uint64_t *key_base;  // [nsets + 1] global key index of each set
@@ -59,23 +74,42 @@ struct MapArgs {
     uint32_t buckets;
     uint64_t total_keys;
     const uint32_t *fulcs;     // [2048]
-    uint32_t *counts;          // [M * kSub] K1: zeroed counts;  K3: cursors (start = record offset)
+    uint32_t *counts;          // [M * stride] K1: zeroed counts;  K3: cursors (start = record offset)
     uint4 *mapped;             // strings: [total] {global partition, bucket, lower1, lower2}
     uint4 *debug_keys;         // [total] hashed Keys (debug builds) or null
     uint2 *lowers;             // K3 output [total]
     uint16_t *bkt;             // K3 output [total]
     unsigned long long *err;   // [nsets]
+    uint32_t M;                // global partitions
+    uint32_t stride;           // MapPlan::stride
+    uint64_t chunk;            // MapPlan::chunk
 };
 
+// Two-pass partition of the records (kernels_part.cu).
+constexpr int kPartThreads = 512;
+constexpr int kPartItems = 8;
+constexpr int kPartTile = kPartThreads * kPartItems;  // records per tile
+constexpr uint32_t kMaxBins = 512;                    // coarse bins of pass 1 (upper bound)
+constexpr uint32_t kTargetBins = 256;                 // coarse bins aimed for
+constexpr uint32_t kLocalRange = 4096;                // partition ids one pass-2 tile may span
+
+struct PartArgs {
+    uint4 *inter;       // [total] {lower1, lower2, global partition, bucket}, coarse-bin order
+    uint32_t *bincur;   // [nbins] cursors, start = offset of the bin's first partition
+    uint32_t *pcur;     // [M] cursors, start = partition offset
+    uint32_t wshift;    // coarse bin = partition >> wshift
+    uint32_t nbins;     // ceil(M / 2^wshift) <= kMaxBins
+};
+// Smallest shift giving at most kTargetBins coarse bins.
+uint32_t part_wshift(uint64_t partitions);
+
 struct ScanArgs {
-    const uint32_t *in;              // [m] sub-counter sizes, kSub per partition
+    const uint32_t *in;              // [m] count matrix, partition-major
     uint32_t *out;                   // [m + 1] exclusive prefix, out[m] = total
-    uint32_t *cursor;                // [m] copy of out[0..m) (scatter cursors) or null
-    uint32_t m;                      // partitions * kSub
-    uint32_t cap;                    // largest allowed partition (sum of its kSub counters)
+    uint32_t *cursor;                // [m] copy of out[0..m) (global-counter scatter cursors) or null
+    uint32_t m;                      // partitions * stride
     unsigned long long *tile_state;  // [tiles], zeroed: (flag << 32) | value
     uint32_t *tile_counter;          // zeroed
-    const uint32_t *part_base;       // [nsets + 1] to name the set of an overflowing partition
     uint32_t nsets;
     unsigned long long *err;         // [nsets]
     unsigned long long wait_ns;      // bound of the look-back wait on a predecessor tile
@@ -86,7 +120,8 @@ struct SearchArgs {
     const uint32_t *part_base;  // [nsets + 1]
     uint32_t nsets;
     uint32_t M;                 // global partitions
-    const uint32_t *G;          // [M * kSub + 1] record offsets; partition g spans [G[g*kSub], G[(g+1)*kSub])
+    const uint32_t *G;          // [M * gstride + 1] record offsets; partition g spans [G[g*gstride], G[(g+1)*gstride])
+    uint32_t gstride;
     const uint2 *lowers;        // partition-contiguous records
     const uint16_t *bkt;
     uint2 *sorted;              // scratch, same indexing as lowers
@@ -134,9 +169,17 @@ size_t search_warp_smem(uint32_t buckets, uint32_t cap);
 // Warps (= partitions in flight) per K4 CTA; 0 when one warp's state does not fit.
 int search_warps_per_cta(uint32_t buckets, uint32_t cap);
 
-cudaError_t launch_map_count(int kind, const MapArgs &a, int grid, cudaStream_t st);
-cudaError_t launch_scatter(int kind, const MapArgs &a, int grid, cudaStream_t st);
+cudaError_t launch_map_count(int kind, const MapArgs &a, const MapPlan &plan, cudaStream_t st);
+cudaError_t launch_scatter(int kind, const MapArgs &a, const MapPlan &plan, cudaStream_t st);
 cudaError_t launch_scan(const ScanArgs &a, cudaStream_t st);
+// Partition sizes out[(g+1)*stride] - out[g*stride] checked against cap (the search
+// bitmap capacity); an oversized partition is reported as PHOBIC_ERR_PARTITION_OVERFLOW.
+// With a PartArgs (else null) it also seeds the partition and bin cursors.
+cudaError_t launch_check_sizes(const uint32_t *out, uint32_t M, uint32_t stride, uint32_t cap,
+                               const uint32_t *part_base, uint32_t nsets, unsigned long long *err,
+                               const PartArgs *part, cudaStream_t st);
+// K3, two passes (pass 1 hashes the keys again, or reads K1's mapped records for strings).
+cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int sm_count, cudaStream_t st);
 // The scan with its first `skip` tile ids never handed out, so the tiles after them
 // wait on predecessors that never publish: the bounded wait must end in
 // PHOBIC_ERR_TIMEOUT (failure-detection tests).

@@ -6,13 +6,16 @@
 // (key_mapping.glsl:43-45) and bucket (:34-41), and counted per partition.
 //
 // K3 replaces apply_partition_offset.comp:9-18 and redistribute_keys.comp:21-53:
-// each key's (lower1, lower2) pair and bucket id are appended to its partition
-// through one of the partition's kSub cursors (chosen by the key index) that K2
-// set to the start of that cursor's slot range.  Appending in arrival order keeps
-// every write front inside one or two L2 sectors, so the scattered 8-byte and
-// 2-byte stores merge in L2 before they reach HBM; spreading a partition over
-// kSub cursors keeps same-address atomics from queueing behind each other.  The bucket order inside a partition is produced later, in
-// shared memory, by K4.
+// each key's (lower1, lower2) pair and bucket id are appended to its partition.
+// The bucket order inside a partition is produced later, in shared memory, by K4.
+//
+// Two plans (plan_map):
+//   chunked  CTA c counts (K1) and places (K3) the keys of one contiguous chunk
+//            with a shared-memory counter per partition; the only global traffic
+//            is the streamed keys, one column of the count matrix and the record
+//            stores.  Used while all partitions' counters fit in shared memory.
+//   global   one counter per partition in global memory, a reduction per key in
+//            K1 and an atomic add per key in K3 (builds with more partitions).
 #include "kernels.cuh"
 
 namespace phobicb200 {
@@ -45,6 +48,23 @@ struct SetCache {
 // loads and atomics are in flight together; the warp's loads stay coalesced.
 constexpr int kUnroll = 4;
 
+// Partition, bucket and lower pair of global key g.
+template <int KIND, bool READ_MAPPED>
+__device__ __forceinline__ void map_key(const MapArgs &a, SetCache &c, const uint32_t *sf, uint64_t g, uint32_t &gp,
+                                        uint32_t &b, uint32_t &l1, uint32_t &l2) {
+    if constexpr (READ_MAPPED) {
+        uint4 r = a.mapped[g];
+        gp = r.x, b = r.y, l1 = r.z, l2 = r.w;
+    } else {
+        c.locate(a, g);
+        Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
+        gp = c.part_base + partition_of(k.partitioner, c.partitions);
+        b = bucket_of(k.bucketer, sf);
+        l1 = k.lower1, l2 = k.lower2;
+    }
+}
+
+// Global plan: grid-stride over all keys, one global counter per partition.
 template <int KIND, bool SCATTER>
 __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     __shared__ uint32_t sf[kFulcrums];
@@ -63,18 +83,12 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
             const uint64_t g = g0 + u * stride;
             gp[u] = 0xFFFFFFFFu;
             if (g >= a.total_keys) continue;
-            if constexpr (kReadMapped) {
-                uint4 r = a.mapped[g];
-                gp[u] = r.x, b[u] = r.y, l1[u] = r.z, l2[u] = r.w;
-            } else {
-                c.locate(a, g);
-                Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
-                gp[u] = c.part_base + partition_of(k.partitioner, c.partitions);
-                b[u] = bucket_of(k.bucketer, sf);
-                l1[u] = k.lower1, l2[u] = k.lower2;
-                if (!SCATTER) {
-                    if (b[u] >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = c.s;
-                    if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+            map_key<KIND, kReadMapped>(a, c, sf, g, gp[u], b[u], l1[u], l2[u]);
+            if (!SCATTER) {
+                if (b[u] >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = c.s;
+                if (a.debug_keys) {
+                    Key4 k = load_key<KIND>(c.data, c.offsets, g - c.lo);
+                    a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
                 }
             }
         }
@@ -82,8 +96,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
             uint32_t slot[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; u++)
-                if (gp[u] != 0xFFFFFFFFu)
-                    slot[u] = atomicAdd(&a.counts[(size_t)gp[u] * kSub + ((g0 + u * stride) & (kSub - 1))], 1u);
+                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&a.counts[gp[u]], 1u);
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
@@ -94,7 +107,7 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
-                atomicAdd(&a.counts[(size_t)gp[u] * kSub + ((g0 + u * stride) & (kSub - 1))], 1u);
+                atomicAdd(&a.counts[gp[u]], 1u);
                 if (KIND == PHOBIC_KEYS_STRINGS) a.mapped[g0 + u * stride] = make_uint4(gp[u], b[u], l1[u], l2[u]);
             }
         }
@@ -102,24 +115,123 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
 }
 
-template <bool SCATTER>
-static cudaError_t launch_map(int kind, const MapArgs &a, int grid, cudaStream_t st) {
-    if (a.total_keys == 0) return cudaSuccess;
-    switch (kind) {
-    case PHOBIC_KEYS_U64: k_map<PHOBIC_KEYS_U64, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
-    case PHOBIC_KEYS_BYTES16: k_map<PHOBIC_KEYS_BYTES16, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
-    case PHOBIC_KEYS_PREHASHED: k_map<PHOBIC_KEYS_PREHASHED, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
-    default: k_map<PHOBIC_KEYS_STRINGS, SCATTER><<<grid, kMapThreads, 0, st>>>(a); break;
+// Chunked plan: CTA c owns keys [c * chunk, (c + 1) * chunk).  K1 counts them per
+// partition in shared memory and writes column c of the count matrix; K3 loads
+// column c of its exclusive scan as cursors and hands out slots with
+// shared-memory atomics.
+template <int KIND, bool SCATTER>
+__global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint32_t *sf = smem;               // [kFulcrums]
+    uint32_t *cnt = smem + kFulcrums;  // [M]
+    constexpr bool kReadMapped = SCATTER && KIND == PHOBIC_KEYS_STRINGS;
+    const uint32_t c = blockIdx.x;
+    if (!kReadMapped)
+        for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
+    for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) cnt[g] = SCATTER ? a.counts[(size_t)g * a.stride + c] : 0u;
+    __syncthreads();
+
+    const uint64_t lo = (uint64_t)c * a.chunk;
+    const uint64_t hi = lo + a.chunk < a.total_keys ? lo + a.chunk : a.total_keys;
+    SetCache sc;
+    uint32_t bad_set = 0xFFFFFFFFu;
+    for (uint64_t g0 = lo + threadIdx.x; g0 < hi; g0 += (uint64_t)kUnroll * kChunkThreads) {
+        uint32_t gp[kUnroll], b[kUnroll], l1[kUnroll], l2[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; u++) {
+            const uint64_t g = g0 + (uint64_t)u * kChunkThreads;
+            gp[u] = 0xFFFFFFFFu;
+            if (g >= hi) continue;
+            map_key<KIND, kReadMapped>(a, sc, sf, g, gp[u], b[u], l1[u], l2[u]);
+            if (!SCATTER) {
+                if (b[u] >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = sc.s;
+                if (a.debug_keys) {
+                    Key4 k = load_key<KIND>(sc.data, sc.offsets, g - sc.lo);
+                    a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+                }
+            }
+        }
+        if constexpr (SCATTER) {
+            uint32_t slot[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++)
+                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&cnt[gp[u]], 1u);
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                if (gp[u] == 0xFFFFFFFFu) continue;
+                a.lowers[slot[u]] = make_uint2(l1[u], l2[u]);
+                a.bkt[slot[u]] = (uint16_t)b[u];
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                if (gp[u] == 0xFFFFFFFFu) continue;
+                atomicAdd(&cnt[gp[u]], 1u);
+                if (KIND == PHOBIC_KEYS_STRINGS)
+                    a.mapped[g0 + (uint64_t)u * kChunkThreads] = make_uint4(gp[u], b[u], l1[u], l2[u]);
+            }
+        }
+    }
+    if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
+    if (!SCATTER) {
+        __syncthreads();
+        for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) a.counts[(size_t)g * a.stride + c] = cnt[g];
+    }
+}
+
+static size_t chunk_smem(uint64_t partitions) { return 4 * ((size_t)kFulcrums + (size_t)partitions); }
+
+MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count) {
+    MapPlan p{};
+    if (partitions <= kChunkMaxPartitions && total_keys > 0) {
+        uint64_t ctas = (total_keys + kChunkMinKeys - 1) / kChunkMinKeys;
+        if (ctas > kChunkCtas) ctas = kChunkCtas;
+        p.chunked = true;
+        p.stride = (uint32_t)ctas;
+        p.grid = (uint32_t)ctas;
+        p.chunk = (total_keys + ctas - 1) / ctas;
+    } else {
+        p.chunked = false;
+        p.stride = 1;
+        uint64_t want = (total_keys + kMapThreads - 1) / kMapThreads;
+        uint64_t cap = (uint64_t)(sm_count > 0 ? sm_count : 148) * 8;
+        p.grid = (uint32_t)(want < cap ? (want ? want : 1) : cap);
+        p.chunk = 0;
+    }
+    return p;
+}
+
+template <bool SCATTER, int KIND>
+static cudaError_t launch_kind(const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    if (plan.chunked) {
+        const size_t smem = chunk_smem(a.M);
+        cudaError_t e = cudaFuncSetAttribute(k_chunk<KIND, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        k_chunk<KIND, SCATTER><<<plan.grid, kChunkThreads, smem, st>>>(a);
+    } else {
+        k_map<KIND, SCATTER><<<plan.grid, kMapThreads, 0, st>>>(a);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_map_count(int kind, const MapArgs &a, int grid, cudaStream_t st) {
-    return launch_map<false>(kind, a, grid, st);
+template <bool SCATTER>
+static cudaError_t launch_map(int kind, const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    if (a.total_keys == 0) return cudaSuccess;
+    switch (kind) {
+    case PHOBIC_KEYS_U64: return launch_kind<SCATTER, PHOBIC_KEYS_U64>(a, plan, st);
+    case PHOBIC_KEYS_BYTES16: return launch_kind<SCATTER, PHOBIC_KEYS_BYTES16>(a, plan, st);
+    case PHOBIC_KEYS_PREHASHED: return launch_kind<SCATTER, PHOBIC_KEYS_PREHASHED>(a, plan, st);
+    default: return launch_kind<SCATTER, PHOBIC_KEYS_STRINGS>(a, plan, st);
+    }
 }
 
-cudaError_t launch_scatter(int kind, const MapArgs &a, int grid, cudaStream_t st) {
-    return launch_map<true>(kind, a, grid, st);
+cudaError_t launch_map_count(int kind, const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    return launch_map<false>(kind, a, plan, st);
+}
+
+cudaError_t launch_scatter(int kind, const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    return launch_map<true>(kind, a, plan, st);
 }
 
 }  // namespace phobicb200

@@ -1,0 +1,252 @@
+// K3 as a two-pass radix partition: keys -> partition-contiguous records.
+//
+// Replaces apply_partition_offset.comp:9-18 and redistribute_keys.comp:21-53 up
+// to the order inside a partition (K4 sorts a partition by bucket in shared
+// memory).  One scattered store per key, as in a single pass with a cursor per
+// partition, leaves HBM and L2 doing 8- and 2-byte partial-sector writes; here
+// every store is part of a contiguous run:
+//
+//   pass 1 (k_bin)    a tile of kPartTile keys is hashed, counting-sorted in
+//                     shared memory by coarse bin (gp >> wshift, at most kMaxBins
+//                     bins of 2^wshift partitions) and written bin by bin to the
+//                     record array `inter`, each run at a bin cursor taken with
+//                     one global atomic per (tile, bin).
+//   pass 2 (k_place)  a tile of `inter` (one or two coarse bins) is
+//                     counting-sorted by partition and written run by run to
+//                     `lowers` / `bkt`, each run at a partition cursor taken with
+//                     one global atomic per (tile, partition).  A tile whose
+//                     partitions span more than kLocalRange ids (only for tiny
+//                     partitions) places its records one atomic at a time.
+//
+// The cursors start at the partition offsets of K2 (bin cursor = offset of the
+// bin's first partition), so the records of partition g fill exactly
+// [G[g], G[g + 1]); their order inside the partition is unspecified, which the
+// search does not depend on.
+#include "kernels.cuh"
+
+namespace phobicb200 {
+
+namespace {
+
+struct SetCache {
+    uint32_t s = 0xFFFFFFFFu;
+    uint64_t lo = 0, hi = 0;
+    const void *data = nullptr;
+    const uint64_t *offsets = nullptr;
+    uint32_t part_base = 0, partitions = 0;
+
+    __device__ __forceinline__ void locate(const MapArgs &a, uint64_t g) {
+        if (g >= lo && g < hi) return;
+        s = a.nsets == 1 ? 0u : find_set(a.key_base, a.nsets, g);
+        const SetDesc &d = a.sets[s];
+        lo = d.key_base;
+        hi = d.key_base + d.n;
+        data = d.data;
+        offsets = d.offsets;
+        part_base = d.part_base;
+        partitions = d.partitions;
+    }
+};
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t t = __shfl_up_sync(kFullMask, v, d);
+        if (lane >= d) v += t;
+    }
+    return v;
+}
+
+// Exclusive prefix of cnt[0, count) into off[0, count), count <= kPartThreads * 8;
+// every thread of the block calls it.  `warp_sums` has kPartThreads / 32 words.
+__device__ __forceinline__ void block_exclusive_scan(const uint32_t *cnt, uint32_t *off, uint32_t count,
+                                                     uint32_t *warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int kWarps = kPartThreads / 32;
+    const uint32_t first = threadIdx.x * 8;
+    uint32_t v[8], sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        v[j] = first + j < count ? cnt[first + j] : 0u;
+        sum += v[j];
+    }
+    const uint32_t incl = warp_incl_scan(sum, lane);
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kWarps ? warp_sums[lane] : 0u;
+        uint32_t wi = warp_incl_scan(w, lane);
+        if (lane < kWarps) warp_sums[lane] = wi - w;
+    }
+    __syncthreads();
+    uint32_t run = warp_sums[warp] + incl - sum;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        if (first + j < count) off[first + j] = run;
+        run += v[j];
+    }
+    __syncthreads();
+}
+
+}  // namespace
+
+size_t part_smem_bytes() { return sizeof(uint4) * kPartTile; }
+
+// Pass 1.  Shared memory: fulcrums (static), bin counters and bases (static),
+// the staged tile (dynamic).
+template <int KIND>
+__global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) {
+    __shared__ uint32_t sf[kFulcrums];
+    __shared__ uint32_t hist[kMaxBins], loff[kMaxBins], gbase[kMaxBins];
+    __shared__ uint32_t warp_sums[kPartThreads / 32];
+    extern __shared__ __align__(16) uint4 stage[];
+    constexpr bool kReadMapped = KIND == PHOBIC_KEYS_STRINGS;
+    if (!kReadMapped)
+        for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
+    const uint64_t tiles = (a.total_keys + kPartTile - 1) / kPartTile;
+    SetCache sc;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t t0 = t * kPartTile;
+        const uint32_t count = (uint32_t)(a.total_keys - t0 < (uint64_t)kPartTile ? a.total_keys - t0 : kPartTile);
+        for (uint32_t i = threadIdx.x; i < p.nbins; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        uint4 rec[kPartItems];
+        uint32_t rank[kPartItems];
+#pragma unroll
+        for (int j = 0; j < kPartItems; j++) {
+            const uint32_t q = j * kPartThreads + threadIdx.x;
+            rank[j] = 0xFFFFFFFFu;
+            if (q >= count) continue;
+            const uint64_t g = t0 + q;
+            if constexpr (kReadMapped) {
+                uint4 r = a.mapped[g];  // {gp, bucket, lower1, lower2}
+                rec[j] = make_uint4(r.z, r.w, r.x, r.y);
+            } else {
+                sc.locate(a, g);
+                Key4 k = load_key<KIND>(sc.data, sc.offsets, g - sc.lo);
+                rec[j] = make_uint4(k.lower1, k.lower2, sc.part_base + partition_of(k.partitioner, sc.partitions),
+                                    bucket_of(k.bucketer, sf));
+            }
+            rank[j] = atomicAdd(&hist[rec[j].z >> p.wshift], 1u);
+        }
+        __syncthreads();
+        block_exclusive_scan(hist, loff, p.nbins, warp_sums);
+        for (uint32_t b = threadIdx.x; b < p.nbins; b += blockDim.x)
+            if (hist[b]) gbase[b] = atomicAdd(&p.bincur[b], hist[b]) - loff[b];
+#pragma unroll
+        for (int j = 0; j < kPartItems; j++)
+            if (rank[j] != 0xFFFFFFFFu) stage[loff[rec[j].z >> p.wshift] + rank[j]] = rec[j];
+        __syncthreads();
+        for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
+            const uint4 r = stage[q];
+            p.inter[gbase[r.z >> p.wshift] + q] = r;
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 2.
+__global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t total, uint2 *lowers, uint16_t *bkt) {
+    __shared__ uint32_t hist[kLocalRange], base[kLocalRange];
+    __shared__ uint32_t warp_sums[kPartThreads / 32];
+    __shared__ uint32_t s_min, s_max;
+    extern __shared__ __align__(16) uint4 stage[];
+    const uint64_t tiles = (total + kPartTile - 1) / kPartTile;
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t t0 = t * kPartTile;
+        const uint32_t count = (uint32_t)(total - t0 < (uint64_t)kPartTile ? total - t0 : kPartTile);
+        if (threadIdx.x == 0) s_min = 0xFFFFFFFFu, s_max = 0;
+        __syncthreads();
+        uint4 rec[kPartItems];
+        uint32_t lo = 0xFFFFFFFFu, hi = 0;
+#pragma unroll
+        for (int j = 0; j < kPartItems; j++) {
+            const uint32_t q = j * kPartThreads + threadIdx.x;
+            if (q >= count) continue;
+            rec[j] = p.inter[t0 + q];
+            lo = min(lo, rec[j].z);
+            hi = max(hi, rec[j].z);
+        }
+        lo = __reduce_min_sync(kFullMask, lo);
+        hi = __reduce_max_sync(kFullMask, hi);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_min, lo);
+            atomicMax(&s_max, hi);
+        }
+        __syncthreads();
+        const uint32_t gmin = s_min, range = s_max - s_min + 1;
+        if (range > kLocalRange) {  // partitions too small for runs: one atomic per record
+#pragma unroll
+            for (int j = 0; j < kPartItems; j++) {
+                const uint32_t q = j * kPartThreads + threadIdx.x;
+                if (q >= count) continue;
+                const uint32_t dst = atomicAdd(&p.pcur[rec[j].z], 1u);
+                lowers[dst] = make_uint2(rec[j].x, rec[j].y);
+                bkt[dst] = (uint16_t)rec[j].w;
+            }
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t i = threadIdx.x; i < range; i += blockDim.x) hist[i] = 0;
+        __syncthreads();
+        uint32_t rank[kPartItems];
+#pragma unroll
+        for (int j = 0; j < kPartItems; j++) {
+            const uint32_t q = j * kPartThreads + threadIdx.x;
+            rank[j] = q < count ? atomicAdd(&hist[rec[j].z - gmin], 1u) : 0xFFFFFFFFu;
+        }
+        __syncthreads();
+        block_exclusive_scan(hist, base, range, warp_sums);  // base = local offsets for now
+#pragma unroll
+        for (int j = 0; j < kPartItems; j++)
+            if (rank[j] != 0xFFFFFFFFu) stage[base[rec[j].z - gmin] + rank[j]] = rec[j];
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < range; i += blockDim.x)
+            if (hist[i]) base[i] = atomicAdd(&p.pcur[gmin + i], hist[i]) - base[i];
+        __syncthreads();
+        for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
+            const uint4 r = stage[q];
+            const uint32_t dst = base[r.z - gmin] + q;
+            lowers[dst] = make_uint2(r.x, r.y);
+            bkt[dst] = (uint16_t)r.w;
+        }
+        __syncthreads();
+    }
+}
+
+uint32_t part_wshift(uint64_t partitions) {
+    uint32_t w = 0;
+    while (((partitions + (1ull << w) - 1) >> w) > kTargetBins) w++;
+    return w;
+}
+
+template <int KIND>
+static cudaError_t launch_bin_kind(const MapArgs &a, const PartArgs &p, int grid, cudaStream_t st) {
+    const size_t smem = part_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_bin<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_bin<KIND><<<grid, kPartThreads, smem, st>>>(a, p);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int sm_count, cudaStream_t st) {
+    if (a.total_keys == 0) return cudaSuccess;
+    const uint64_t tiles = (a.total_keys + kPartTile - 1) / kPartTile;
+    const uint64_t cap = (uint64_t)(sm_count > 0 ? sm_count : 148) * 2;
+    const int grid = (int)(tiles < cap ? tiles : cap);
+    cudaError_t e;
+    switch (kind) {
+    case PHOBIC_KEYS_U64: e = launch_bin_kind<PHOBIC_KEYS_U64>(a, p, grid, st); break;
+    case PHOBIC_KEYS_BYTES16: e = launch_bin_kind<PHOBIC_KEYS_BYTES16>(a, p, grid, st); break;
+    case PHOBIC_KEYS_PREHASHED: e = launch_bin_kind<PHOBIC_KEYS_PREHASHED>(a, p, grid, st); break;
+    default: e = launch_bin_kind<PHOBIC_KEYS_STRINGS>(a, p, grid, st); break;
+    }
+    if (e != cudaSuccess) return e;
+    const size_t smem = part_smem_bytes();
+    e = cudaFuncSetAttribute(k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_place<<<grid, kPartThreads, smem, st>>>(p, a.total_keys, a.lowers, a.bkt);
+    return cudaGetLastError();
+}
+
+}  // namespace phobicb200

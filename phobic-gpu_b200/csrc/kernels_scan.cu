@@ -4,9 +4,10 @@
 // prefix_sum_offset.comp:13-19, driven by PrefixSumStage::addCommands,
 // src/prefix_sum_stage.cpp:42-86) and the host's leading zero
 // (include/phobicGpu/mphf_builder.h:254-257): out[0] = 0, out[p + 1] = out[p] + size[p].
-// It also seeds the scatter cursors of K3 (a copy of the exclusive prefix) and
-// checks every partition against the search bitmap capacity, which the
-// reference leaves unchecked (search.comp:21).
+// The scanned array is the (partition, chunk) count matrix of K1, so the prefix
+// is at once every partition's record offset and every chunk's scatter cursor.
+// A second small kernel checks every partition against the search bitmap
+// capacity, which the reference leaves unchecked (search.comp:21).
 //
 // Each CTA takes the next tile id from a counter, so every tile it waits on was
 // started before it; the wait on a predecessor is still bounded in time
@@ -40,7 +41,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
     if ((uint64_t)tile * kScanTile >= a.m) return;  // only when tile ids were skipped on purpose
     const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
 
-    static_assert(kScanItems == kSub, "one thread holds the kSub counters of one partition");
     uint32_t v[kScanItems];
     uint32_t sum = 0;
 #pragma unroll
@@ -48,11 +48,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(ScanArgs a) {
         uint64_t idx = base + j;
         v[j] = idx < a.m ? a.in[idx] : 0u;
         sum += v[j];
-    }
-    if (sum > a.cap) {  // this thread's items are the sub-counters of partition base / kSub
-        const uint32_t part = (uint32_t)(base / kSub);
-        uint32_t set = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, part);
-        report_error(&a.err[set], part - a.part_base[set], PHOBIC_ERR_PARTITION_OVERFLOW);
     }
 
     uint32_t incl = warp_incl_scan(sum, lane);
@@ -116,6 +111,32 @@ cudaError_t launch_scan(const ScanArgs &a, cudaStream_t st) {
     ScanArgs b = a;
     if (!b.wait_ns) b.wait_ns = kSpinTimeoutNs;
     k_scan<<<tiles, kScanThreads, 0, st>>>(b);
+    return cudaGetLastError();
+}
+
+__global__ void k_check_sizes(const uint32_t *out, uint32_t M, uint32_t stride, uint32_t cap, const uint32_t *part_base,
+                              uint32_t nsets, unsigned long long *err, PartArgs part, bool seed) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= M) return;
+    const uint32_t start = out[(size_t)g * stride];
+    if (seed) {
+        part.pcur[g] = start;
+        if ((g & ((1u << part.wshift) - 1)) == 0) part.bincur[g >> part.wshift] = start;
+    }
+    const uint32_t size = out[(size_t)(g + 1) * stride] - start;
+    if (size > cap) {
+        const uint32_t set = nsets == 1 ? 0u : find_set(part_base, nsets, g);
+        report_error(&err[set], g - part_base[set], PHOBIC_ERR_PARTITION_OVERFLOW);
+    }
+}
+
+cudaError_t launch_check_sizes(const uint32_t *out, uint32_t M, uint32_t stride, uint32_t cap,
+                               const uint32_t *part_base, uint32_t nsets, unsigned long long *err,
+                               const PartArgs *part, cudaStream_t st) {
+    if (M == 0) return cudaSuccess;
+    PartArgs p{};
+    if (part) p = *part;
+    k_check_sizes<<<(M + 255) / 256, 256, 0, st>>>(out, M, stride, cap, part_base, nsets, err, p, part != nullptr);
     return cudaGetLastError();
 }
 

@@ -53,7 +53,7 @@ __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B 
 // so the uint2 staging array kl is 8-byte aligned:
 //   union of
 //     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
-//     search phase:  hs [260] slots (256 keys + 3 padding copies of slot 0),
+//     search phase:  hs [260] packed slots (256 keys, padded to a multiple of 4),
 //                    kl uint2[256] keys of a large bucket
 //   sched [B]        search schedule, in search order: start | size << 16
 //   order [B/2]      bucket id (u16) in search order
@@ -127,30 +127,38 @@ __device__ __forceinline__ uint32_t lds32_next(uint32_t addr) {
     asm volatile("ld.shared.u32 %0, [%1+4];" : "=r"(v) : "r"(addr));
     return v;
 }
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+    uint4 v;
+    asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
+    return v;
+}
 
-// Smallest free offset in rounds of 1024 (see the offset search above).  Keys are
-// consumed in unrolled groups of 4; SlotOf(i) returns key i's slot for i < s + 3,
-// where slots past the last key repeat key 0 (OR is idempotent).  A round stops
-// early once every lane's window holds an occupied slot.  The bitmap is addressed
-// through 32-bit shared-memory addresses: lane base + 4 * (slot >> 5).
-template <typename SlotOf>
-__device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, uint32_t s, uint32_t ps, int lane,
-                                                      SlotOf slot_of) {
+// A slot h as the offset search reads it: the byte offset of its bitmap word,
+// 4 * (h >> 5), shifted left by 5, with the bit position h & 31 in the low bits.
+// The funnel shift only looks at the low 5 bits, so one word serves both uses.
+__device__ __forceinline__ uint32_t pack_slot(uint32_t h) { return ((h >> 5) << 7) | (h & 31); }
+__device__ __forceinline__ uint32_t unpack_slot(uint32_t v) { return ((v >> 7) << 5) | (v & 31); }
+
+// Smallest free offset in rounds of 1024 (see the offset search above).  hs holds
+// the s packed slots of the bucket, 16-byte aligned, padded to a multiple of 4
+// with copies of slot 0 (OR is idempotent); each group of 4 is one broadcast
+// 128-bit load.  A round stops early once every lane's window holds an occupied
+// slot.  The bitmap is addressed through 32-bit shared-memory addresses.
+__device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, const uint32_t *hs, uint32_t s,
+                                                      uint32_t ps, int lane) {
     const uint32_t occ_sa = (uint32_t)__cvta_generic_to_shared(occ);
+    const uint32_t hs_sa = (uint32_t)__cvta_generic_to_shared(hs);
     for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
         const uint32_t w = w0 + 32 * lane;
         const bool live = w < ps;
         const uint32_t base = occ_sa + (live ? (w >> 3) : 0u);
         uint32_t bad = live ? 0u : kFullMask;
         for (uint32_t i = 0; i < s; i += 4) {
-            uint32_t h[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) h[u] = slot_of(i + u);
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const uint32_t a = base + ((h[u] >> 5) << 2);
-                bad |= __funnelshift_r(lds32(a), lds32_next(a), h[u]);
-            }
+            const uint4 v = lds128(hs_sa + 4 * i);
+            const uint32_t a0 = base + (v.x >> 5), a1 = base + (v.y >> 5);
+            const uint32_t a2 = base + (v.z >> 5), a3 = base + (v.w >> 5);
+            bad |= __funnelshift_r(lds32(a0), lds32_next(a0), v.x) | __funnelshift_r(lds32(a1), lds32_next(a1), v.y);
+            bad |= __funnelshift_r(lds32(a2), lds32_next(a2), v.z) | __funnelshift_r(lds32(a3), lds32_next(a3), v.w);
             if (__all_sync(kFullMask, bad == kFullMask)) break;
         }
         uint32_t valid = ~bad;
@@ -165,9 +173,10 @@ __device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, uint3
 }
 
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
-__device__ __forceinline__ uint32_t place_small(uint32_t *occ, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
+__device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
                                                 uint32_t k_lim, int lane, uint32_t *pilot) {
     const bool mine = lane < (int)s;
+    const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
         if (k == kDupCheckAt && s > 1) {
             bool d = false;
@@ -182,12 +191,15 @@ __device__ __forceinline__ uint32_t place_small(uint32_t *occ, uint2 L, uint32_t
             uint32_t m = __match_any_sync(kFullMask, h);
             if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
         }
-        const uint32_t hp = __shfl_sync(kFullMask, h, mine ? lane : 0);
-        const uint32_t o = first_free_offset(occ, s, ps, lane, [&](uint32_t j) { return __shfl_sync(kFullMask, hp, j); });
+        const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
+        if (lane < (int)padded) ws.hs[lane] = hp;
+        __syncwarp();
+        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+        __syncwarp();
         if (o == kNone) continue;
         if (mine) {
             uint32_t q = h + o;
-            mark(occ, q >= ps ? q - ps : q, ps);
+            mark(ws.occ, q >= ps ? q - ps : q, ps);
         }
         __syncwarp();
         *pilot = o + ps * k;
@@ -201,6 +213,7 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
                                                 FastMod fm, uint32_t k_lim, int lane, uint32_t *pilot) {
     for (uint32_t i = lane; i < s; i += 32) ws.kl[i] = src[i];
     __syncwarp();
+    const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
         if (k == kDupCheckAt) {
             bool d = false;
@@ -214,21 +227,21 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
         for (uint32_t i = lane; i < s; i += 32) {
             uint2 key = ws.kl[i];
             uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
-            ws.hs[i] = h;
+            ws.hs[i] = pack_slot(h);
             uint32_t bit = 1u << (h & 31);
             d |= (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
         }
         const bool dup = __any_sync(kFullMask, d);
-        for (uint32_t i = lane; i < s; i += 32) ws.scr[ws.hs[i] >> 5] = 0;
+        for (uint32_t i = lane; i < s; i += 32) ws.scr[unpack_slot(ws.hs[i]) >> 5] = 0;
         __syncwarp();
         if (dup) continue;
-        if (lane < 3) ws.hs[s + lane] = ws.hs[0];
+        if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
         __syncwarp();
-        const uint32_t *hs = ws.hs;
-        const uint32_t o = first_free_offset(ws.occ, s, ps, lane, [&](uint32_t j) { return hs[j]; });
+        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+        __syncwarp();
         if (o == kNone) continue;
         for (uint32_t i = lane; i < s; i += 32) {
-            uint32_t q = ws.hs[i] + o;
+            uint32_t q = unpack_slot(ws.hs[i]) + o;
             mark(ws.occ, q >= ps ? q - ps : q, ps);
         }
         __syncwarp();
@@ -242,9 +255,9 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
 __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
                                                      uint32_t g, uint32_t p, int lane) {
     const uint32_t B = a.buckets;
-    const uint32_t base = a.G[(size_t)g * kSub];
-    const uint32_t ps = a.G[(size_t)(g + 1) * kSub] - base;
-    if (ps > a.cap) return PHOBIC_OK;  // reported by the scan
+    const uint32_t base = a.G[(size_t)g * a.gstride];
+    const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
+    if (ps > a.cap) return PHOBIC_OK;  // reported by the size check
     const uint32_t ow = occ_words(a.cap);
     uint32_t *pil = d.pilots + p;
     const size_t pstride = d.partitions;
@@ -344,7 +357,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
             L_next = lane < (int)(sc_next >> 16) ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
         }
         uint32_t pilot = 0;
-        const uint32_t st_code = s <= 32 ? place_small(ws.occ, L, s, ps, fm, k_lim, lane, &pilot)
+        const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, lane, &pilot)
                                          : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
         if (st_code != PHOBIC_OK) return st_code;
         if (lane == 0) pil[(size_t)b * pstride] = pilot;
@@ -363,7 +376,7 @@ int search_warps_per_cta(uint32_t buckets, uint32_t cap) {
 }
 
 __global__ void __launch_bounds__(kSearchWarps * 32, 4) k_search(SearchArgs a) {
-    extern __shared__ uint32_t smem[];
+    extern __shared__ __align__(16) uint32_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const WarpSmem ws = carve(smem + (size_t)warp * warp_words(a.buckets, a.cap), a.buckets, a.cap);
     for (;;) {
@@ -376,9 +389,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 4) k_search(SearchArgs a) {
         const SetDesc &d = a.sets[s];
         const uint32_t p = g - d.part_base;
         if (lane == 0 && d.part_off) {
-            const uint32_t g0 = a.G[(size_t)d.part_base * kSub];
-            d.part_off[p] = a.G[(size_t)g * kSub] - g0;
-            if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[(size_t)(g + 1) * kSub] - g0;
+            const uint32_t g0 = a.G[(size_t)d.part_base * a.gstride];
+            d.part_off[p] = a.G[(size_t)g * a.gstride] - g0;
+            if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[(size_t)(g + 1) * a.gstride] - g0;
         }
         const uint32_t code = search_partition(a, ws, d, g, p, lane);
         if (code != PHOBIC_OK && lane == 0) report_error(&a.err[s], p, code);

@@ -44,9 +44,9 @@ constexpr size_t kOffPartBase = kOffKeyBase + A(16);
 constexpr size_t kOffErr = kOffPartBase + A(8);
 constexpr size_t kOffQueue = kOffErr + A(8);
 constexpr size_t kOffCount = kOffQueue + A(64);
-constexpr size_t kOffG = kOffCount + A(4 * kNoAllocMaxPartitions * kSub);
-constexpr size_t kOffTiles = kOffG + A(4 * (kNoAllocMaxPartitions * kSub + 1));
-constexpr size_t kTilesMax = (kNoAllocMaxPartitions * kSub + kScanTile - 1) / kScanTile;
+constexpr size_t kOffG = kOffCount + A(4 * kNoAllocMaxPartitions);
+constexpr size_t kOffTiles = kOffG + A(4 * (kNoAllocMaxPartitions + 1));
+constexpr size_t kTilesMax = (kNoAllocMaxPartitions + kScanTile - 1) / kScanTile;
 constexpr size_t kOffLowers = kOffTiles + A(8 * kTilesMax + 8);
 constexpr size_t kOffBkt = kOffLowers + A(8 * kNoAllocMaxKeys);
 constexpr size_t kOffSorted = kOffBkt + A(2 * kNoAllocMaxKeys);
@@ -120,7 +120,7 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
     uint2 *d_lowers = reinterpret_cast<uint2 *>(base + kOffLowers);
     uint16_t *d_bkt = reinterpret_cast<uint16_t *>(base + kOffBkt);
     uint2 *d_sorted = reinterpret_cast<uint2 *>(base + kOffSorted);
-    const uint32_t tiles = (uint32_t)((m * kSub + kScanTile - 1) / kScanTile);
+    const uint32_t tiles = (uint32_t)((m + kScanTile - 1) / kScanTile);
 
     // Host-side tables live on the stack; copies from pageable memory are staged by
     // the runtime before cudaMemcpyAsync returns.
@@ -140,17 +140,21 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
               cuda(cudaMemcpyAsync(d_kb, hkb, sizeof(hkb), cudaMemcpyHostToDevice, s)) &&
               cuda(cudaMemcpyAsync(d_pb, hpb, sizeof(hpb), cudaMemcpyHostToDevice, s)) &&
               cuda(cudaMemsetAsync(d_err, 0xFF, 8, s)) && cuda(cudaMemsetAsync(d_queue, 0, 64, s)) &&
-              cuda(cudaMemsetAsync(d_count, 0, 4 * m * kSub, s)) && cuda(cudaMemsetAsync(d_tiles, 0, 8 * tiles + 8, s));
+              cuda(cudaMemsetAsync(d_count, 0, 4 * m, s)) && cuda(cudaMemsetAsync(d_tiles, 0, 8 * tiles + 8, s));
     if (ok && m == 0) ok = cuda(cudaMemsetAsync(result->partition_offsets, 0, 4, s));
     if (ok && n) {
-        const int grid = (int)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)sm_count * 8);
-        MapArgs ma{d_desc, d_kb, 1, B, n, d_fulcs, d_count, nullptr, nullptr, d_lowers, d_bkt, d_err};
-        ScanArgs sa{d_count, d_G, d_count, (uint32_t)(m * kSub), cap, d_tiles,
-                    reinterpret_cast<uint32_t *>(d_tiles + tiles), d_pb, 1, d_err, 0};
-        SearchArgs qa{d_desc, d_pb, 1, (uint32_t)m, d_G, d_lowers, d_bkt, d_sorted, nullptr, B, cap, k_max,
+        // The global-counter plan: one counter per partition keeps the scratch small.
+        const uint32_t grid = (uint32_t)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)sm_count * 8);
+        const MapPlan plan{false, 1, grid, 0};
+        MapArgs ma{d_desc, d_kb, 1, B, n, d_fulcs, d_count, nullptr, nullptr, d_lowers, d_bkt, d_err,
+                   (uint32_t)m, 1, 0};
+        ScanArgs sa{d_count, d_G, d_count, (uint32_t)m, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles), 1,
+                    d_err, 0};
+        SearchArgs qa{d_desc, d_pb, 1, (uint32_t)m, d_G, 1, d_lowers, d_bkt, d_sorted, nullptr, B, cap, k_max,
                       d_queue, d_err};
-        ok = cuda(launch_map_count(keys->kind, ma, grid, s)) && cuda(launch_scan(sa, s)) &&
-             cuda(launch_scatter(keys->kind, ma, grid, s)) && cuda(launch_search(qa, sm_count, s));
+        ok = cuda(launch_map_count(keys->kind, ma, plan, s)) && cuda(launch_scan(sa, s)) &&
+             cuda(launch_check_sizes(d_G, (uint32_t)m, 1, cap, d_pb, 1, d_err, nullptr, s)) &&
+             cuda(launch_scatter(keys->kind, ma, plan, s)) && cuda(launch_search(qa, sm_count, s));
     }
     if (!ok) {
         cudaGetLastError();

@@ -85,8 +85,9 @@ def test_bytes_needed_formula(phobic):
     lib = phobic.lib()
     k = phobic.Keys(phobic.KEYS_U64, 1, 100_000_000, None, None)
     need = lib.phobic_build_bytes_needed(C.byref(k), C.byref(cfg.params))
-    # device-resident u64 keys: lowers 8 + bucket ids 2 + sorted 8 bytes per key, plus pilots and offsets
-    assert 18e8 < need < 20e8
+    # device-resident u64 keys: lowers 8 + bucket ids 2 + partition records 16 bytes per key, plus the
+    # (partition, chunk) count matrix and its prefix, pilots and offsets
+    assert 26e8 < need < 28e8
 
 
 def test_context_without_device_fails_loudly(phobic):
