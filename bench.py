@@ -39,6 +39,10 @@ sys.path.insert(0, str(ROOT / "phobic-gpu_b200"))
 LAMBDA, PSIZE, SEED = 7.0, 2500, 2
 METRIC = "Mkeys/s MPHF build @100M u64 keys; p50/p99 latency, batched vs plain"
 CONFIG_NAME = "plain build, 100M unique u64 keys splitmix64(seed=2), lambda=7.0, alpha=1.0, partition 2500"
+
+
+def workload_name(n: int) -> str:
+    return CONFIG_NAME if n == 100_000_000 else CONFIG_NAME.replace("100M", f"{n:,}")
 # Algorithmic bytes of the search kernel per key: read its (lower1, lower2) record (8 B)
 # and bucket id (2 B), write 4 B of pilot per bucket (1/lambda buckets per key).
 K4_BYTES_PER_KEY = 8 + 2 + 4 / LAMBDA
@@ -99,10 +103,10 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    import ranks
+
+    info = ranks.RankInfo.from_env()
+    return info.world, info.rank, info.local
 
 
 def cpu_baseline(n_sample: int, min_seconds: float = 10.0, max_reps: int = 6) -> dict:
@@ -171,20 +175,16 @@ def run_ours(args) -> None:
     import keygen
     import phobic
 
-    world, rank, local = dist_setup()
+    import ranks
+
+    info = ranks.RankInfo.from_env()
+    world, rank, local = info.world, info.rank, info.local
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
+    grp = ranks.Group(info, "nccl", device="cuda")
 
     n = args.n
     cfg = phobic.MPHFconfig(LAMBDA, PSIZE)
-    keys = keygen.splitmix64(SEED + rank, n)  # every rank: its own independent key set
+    keys = keygen.splitmix64(ranks.rank_seed(SEED, rank), n)  # every rank: its own independent key set
     ctx = phobic.Context(local)
     parts = cfg.partitions(n)
     B = cfg.bucketCountPerPartition
@@ -198,8 +198,7 @@ def run_ours(args) -> None:
     for _ in range(args.warmup):
         ctx.build(dk, cfg, out=(dp, do))
     torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
+    grp.barrier()
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     search_ms = []
     torch.cuda.synchronize()
@@ -211,10 +210,7 @@ def run_ours(args) -> None:
     torch.cuda.synchronize()
     dev_ms = t_start.elapsed_time(t_end)
     stage = dict(r.timings)
-    if pg:
-        t = torch.tensor([dev_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        dev_ms = float(t.item())
+    dev_ms = grp.max(dev_ms)
     ms_per_step = dev_ms / args.steps
     value = world * n / (ms_per_step / 1e3) / 1e6
 
@@ -228,8 +224,7 @@ def run_ours(args) -> None:
     hks = phobic.KeySet(phobic.KEYS_U64, n, hk.data_ptr())
     for _ in range(max(1, args.warmup)):
         ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
-    if pg:
-        pg.barrier()
+    grp.barrier()
     e2e_wall, e2e_dev = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -237,11 +232,7 @@ def run_ours(args) -> None:
         e2e_wall.append(time.perf_counter() - t0)
         e2e_dev.append(r2.timings["total"])
     clocks.__exit__(None, None, None)
-    e2e_ms = 1e3 * sum(e2e_wall) / len(e2e_wall)
-    if pg:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = grp.max(1e3 * sum(e2e_wall) / len(e2e_wall))
     same = bool((hp.numpy() == dp.cpu().numpy()).all())
 
     # ---- host encoding of the result (Mphf::setData), C2's encoder: interleaved dictionary + diff compact
@@ -252,9 +243,7 @@ def run_ours(args) -> None:
 
     if rank != 0:
         ctx.close()
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
+        grp.close()
         return
     peaks = measured_peaks()
     k4_ms = statistics.mean(search_ms)
@@ -269,9 +258,10 @@ def run_ours(args) -> None:
         "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seed 2 + rank)",
-        "config": {"workload": CONFIG_NAME, "n_keys": n, "lambda": LAMBDA, "alpha": 1.0, "partition_size": PSIZE,
+        "config": {"workload": workload_name(n), "n_keys": n, "lambda": LAMBDA, "alpha": 1.0, "partition_size": PSIZE,
                    "buckets_per_partition": B, "partitions": parts, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (800 MB keys per step)"},
+                   "l2": f"inputs larger than L2 ({8 * n / 1e6:,.0f} MB keys per step)" if 8 * n > 126e6
+                   else f"inputs smaller than L2 ({8 * n / 1e6:,.0f} MB keys per step)"},
         "stages_ms": {k: round(v, 4) for k, v in stage.items() if k != "kernels"},
         "bijection_bad": bad, "host_result_equals_device": same,
         "gpu_launches": int(stage["kernels"]) * args.steps,
@@ -290,9 +280,7 @@ def run_ours(args) -> None:
     }
     print(json.dumps(line), flush=True)
     ctx.close()
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    grp.close()
 
 
 # ------------------------------------------------------------------ other workloads

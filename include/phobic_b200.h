@@ -151,7 +151,8 @@ PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *
                                  const phobic_params *params, const phobic_result *results,
                                  phobic_status *statuses, phobic_timings *timings);
 
-/* Failure-detection hook: runs the partition-offset scan with its first tile never
+/* No counterpart in the reference (it has no bounded device waits to test).
+ * Failure-detection hook: runs the partition-offset scan with its first tile never
  * scheduled, so the next tile's look-back waits on a flag that nothing sets.  The
  * kernel's bounded wait (wait_ms) must give up and record PHOBIC_ERR_TIMEOUT, which is
  * returned in *observed; the context stays usable afterwards. */

@@ -30,6 +30,7 @@ constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;  // entries per thread: one tile = 4096 entries
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kSearchWarps = 8;
+constexpr int kSearchCtasPerSm = 4;  // register budget: 65536 / (4 * 256) -> 64 per thread
 constexpr size_t kSearchSmemLimit = 227 * 1024;
 
 // One key set of a build.

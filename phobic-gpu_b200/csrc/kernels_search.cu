@@ -39,7 +39,7 @@ namespace phobicb200 {
 namespace {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
-constexpr uint32_t kHsWords = 260;  // even, so kl after it stays 8-byte aligned
+constexpr uint32_t kHsWords = 260;  // packed slots of up to 256 keys, padded to a multiple of 4
 
 // Occupancy bitmap of a partition of at most cap slots, stored twice in a row
 // (bits [ps, 2 ps) repeat bits [0, ps)) plus one spare word.
@@ -48,55 +48,49 @@ __host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (2
 __host__ __device__ __forceinline__ uint32_t scr_words(uint32_t cap) { return (cap + 31) / 32 + 1; }
 __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B + 1) / 2; }
 
-// Per-warp shared memory, in 32-bit words; every warp's region starts on a
-// 16-byte boundary (its size is rounded up to 4 words) and the union comes first,
-// so the uint2 staging array kl is 8-byte aligned:
+// Per-warp shared memory, in 32-bit words.  Every warp's region starts on a
+// 16-byte boundary (its size is rounded up to 4 words) and the union comes
+// first, so hs is 16-byte aligned for the 128-bit slot loads:
 //   union of
-//     prep phase:    cnt u16[B], cur u16[B], binPos [256], binKey [256]
-//     search phase:  hs [260] packed slots (256 keys, padded to a multiple of 4),
-//                    kl uint2[256] keys of a large bucket
-//   sched [B]        search schedule, in search order: start | size << 16
-//   order [B/2]      bucket id (u16) in search order
+//     prep phase:    cur u16[B] bucket cursors, binPos u16[256], binKey u16[256]
+//     search phase:  hs [260] packed slots, scr [SW] collision scratch of large buckets
+//   cnt   u16[B]     bucket sizes
+//   sched [B]        search schedule, in search order: start | bucket << 16
 //   occ   [OW]       occupied slots, bits [ps, 2 ps) mirror [0, ps)
-//   scr   [SW]       collision scratch of large buckets
-__host__ __device__ __forceinline__ size_t union_words(uint32_t B) {
-    size_t prep = 2 * (size_t)half_words(B) + 512, search = kHsWords + 512;
+__host__ __device__ __forceinline__ size_t union_words(uint32_t B, uint32_t cap) {
+    size_t prep = (size_t)half_words(B) + 256, search = kHsWords + scr_words(cap);
     return prep > search ? prep : search;
 }
 
 __host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
-    size_t w = union_words(B) + (size_t)B + half_words(B) + (size_t)occ_words(cap) + scr_words(cap);
+    size_t w = union_words(B, cap) + half_words(B) + (size_t)B + (size_t)occ_words(cap);
     return (w + 3) & ~size_t(3);
 }
 
 struct WarpSmem {
+    uint32_t *cur32, *binPos, *binKey;  // packed u16 pairs (prep phase)
+    uint32_t *hs, *scr;                 // search phase
+    uint32_t *cnt32;                    // packed u16 pairs
     uint32_t *sched;
-    uint16_t *order;
-    uint32_t *occ, *scr;
-    uint32_t *cnt32, *cur32;  // packed u16 pairs
-    uint16_t *cur16;
-    uint32_t *binPos, *binKey;
-    uint32_t *hs;
-    uint2 *kl;
+    uint32_t *occ;
 };
 
 __device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap) {
     WarpSmem m;
-    m.cnt32 = w;
-    m.cur32 = w + half_words(B);
-    m.cur16 = reinterpret_cast<uint16_t *>(m.cur32);
-    m.binPos = w + 2 * half_words(B);
-    m.binKey = m.binPos + 256;
+    m.cur32 = w;
+    m.binPos = w + half_words(B);
+    m.binKey = m.binPos + 128;
     m.hs = w;
-    m.kl = reinterpret_cast<uint2 *>(w + kHsWords);
-    m.sched = w + union_words(B);
-    m.order = reinterpret_cast<uint16_t *>(m.sched + B);
-    m.occ = m.sched + B + half_words(B);
-    m.scr = m.occ + occ_words(cap);
+    m.scr = w + kHsWords;
+    m.cnt32 = w + union_words(B, cap);
+    m.sched = m.cnt32 + half_words(B);
+    m.occ = m.sched + B;
     return m;
 }
 
 __device__ __forceinline__ uint32_t half_get(const uint32_t *w, uint32_t b) { return (w[b >> 1] >> ((b & 1) << 4)) & 0xFFFFu; }
+// Adds v to the u16 entry b of a packed array (no entry may exceed 0xFFFF).
+__device__ __forceinline__ void half_add_n(uint32_t *w, uint32_t b, uint32_t v) { atomicAdd(&w[b >> 1], v << ((b & 1) << 4)); }
 __device__ __forceinline__ uint32_t half_add(uint32_t *w, uint32_t b) {
     uint32_t sh = (b & 1) << 4;
     return (atomicAdd(&w[b >> 1], 1u << sh) >> sh) & 0xFFFFu;
@@ -208,24 +202,23 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
     return PHOBIC_ERR_SEARCH_LIMIT;
 }
 
-// One bucket of more than 32 keys, staged in shared memory (ws.kl, ws.hs).
+// One bucket of more than 32 keys (a few per partition); its keys are read from
+// the bucket-ordered copy in global memory, slots go to ws.hs.
 __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 *src, uint32_t s, uint32_t ps,
                                                 FastMod fm, uint32_t k_lim, int lane, uint32_t *pilot) {
-    for (uint32_t i = lane; i < s; i += 32) ws.kl[i] = src[i];
-    __syncwarp();
     const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
         if (k == kDupCheckAt) {
             bool d = false;
             for (uint32_t t = 0; t + 1 < s; t++) {
-                uint2 kt = ws.kl[t];
-                for (uint32_t i = lane; i < s; i += 32) d |= i > t && ws.kl[i].x == kt.x && ws.kl[i].y == kt.y;
+                uint2 kt = src[t];
+                for (uint32_t i = lane; i < s; i += 32) d |= i > t && src[i].x == kt.x && src[i].y == kt.y;
             }
             if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
         }
         bool d = false;
         for (uint32_t i = lane; i < s; i += 32) {
-            uint2 key = ws.kl[i];
+            uint2 key = src[i];
             uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
             ws.hs[i] = pack_slot(h);
             uint32_t bit = 1u << (h & 31);
@@ -264,8 +257,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
 
     for (uint32_t i = lane; i < half_words(B); i += 32) ws.cnt32[i] = 0;
     for (uint32_t i = lane; i < ow; i += 32) ws.occ[i] = 0;
-    for (uint32_t i = lane; i < scr_words(a.cap); i += 32) ws.scr[i] = 0;
-    for (uint32_t i = lane; i < 512; i += 32) ws.binPos[i] = 0;
+    for (uint32_t i = lane; i < 256; i += 32) ws.binPos[i] = 0;  // binPos and binKey
     __syncwarp();
 
     // Bucket sizes of this partition (bucket_sizes.comp:21-35).
@@ -280,18 +272,19 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         uint32_t s = half_get(ws.cnt32, b);
         if (a.debug_sizes) a.debug_sizes[(size_t)g * B + b] = s;
         if (s > kMaxBucket) over = true;
-        else if (s) atomicAdd(&ws.binPos[kBins - s], 1u);
+        else if (s) half_add(ws.binPos, kBins - s);
         else pil[(size_t)b * pstride] = 0;
     }
     if (__any_sync(kFullMask, over)) return PHOBIC_ERR_BUCKET_OVERFLOW;
     __syncwarp();
 
-    // Exclusive prefix over bins of bucket counts and key counts (sort_sum.comp:184-215).
+    // Exclusive prefix over bins of bucket counts and key counts (sort_sum.comp:184-215);
+    // lane L owns bins 8L .. 8L+7, i.e. packed words 4L .. 4L+3 of each table.
     uint32_t c[8], loc = 0, lock = 0;
 #pragma unroll
     for (int j = 0; j < 8; j++) {
         uint32_t bin = 8 * lane + j;
-        c[j] = ws.binPos[bin];
+        c[j] = half_get(ws.binPos, bin);
         loc += c[j];
         lock += c[j] * (kBins - bin);
     }
@@ -300,16 +293,18 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     uint32_t ex = inc - loc, exk = inck - lock;
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < 8; j++) {
+    for (int j = 0; j < 8; j += 2) {
         uint32_t bin = 8 * lane + j;
-        ws.binPos[bin] = ex;
-        ws.binKey[bin] = exk;
-        ex += c[j];
-        exk += c[j] * (kBins - bin);
+        const uint32_t ex1 = ex + c[j], exk1 = exk + c[j] * (kBins - bin);
+        ws.binPos[bin >> 1] = ex | (ex1 << 16);
+        ws.binKey[bin >> 1] = exk | (exk1 << 16);
+        ex = ex1 + c[j + 1];
+        exk = exk1 + c[j + 1] * (kBins - bin - 1);
     }
     __syncwarp();
 
     // Search order: within a bin, the higher bucket index first (sort_sum.comp:156).
+    uint16_t *cur16 = reinterpret_cast<uint16_t *>(ws.cur32);
     for (uint32_t c0 = 0; c0 < B; c0 += 32) {
         const int bi = (int)B - 1 - (int)(c0 + lane);
         const uint32_t s = bi >= 0 ? half_get(ws.cnt32, bi) : 0u;
@@ -317,15 +312,14 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         const uint32_t r = __popc(peers & lanemask_lt());
         const uint32_t bin = kBins - s;
         if (s) {
-            const uint32_t j = ws.binPos[bin] + r, st = ws.binKey[bin] + r * s;
-            ws.order[j] = (uint16_t)bi;
-            ws.sched[j] = st | (s << 16);
-            ws.cur16[bi] = (uint16_t)st;
+            const uint32_t j = half_get(ws.binPos, bin) + r, st = half_get(ws.binKey, bin) + r * s;
+            ws.sched[j] = st | ((uint32_t)bi << 16);
+            cur16[bi] = (uint16_t)st;
         }
         __syncwarp();
         if (s && lane == __ffs(peers) - 1) {
-            ws.binPos[bin] += __popc(peers);
-            ws.binKey[bin] += __popc(peers) * s;
+            half_add_n(ws.binPos, bin, __popc(peers));
+            half_add_n(ws.binKey, bin, __popc(peers) * s);
         }
         __syncwarp();
     }
@@ -340,21 +334,25 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     }
     __threadfence_block();
     __syncwarp();
+    // The search-phase half of the union: large buckets expect a clear collision scratch.
+    for (uint32_t i = lane; i < scr_words(a.cap); i += 32) ws.scr[i] = 0;
+    __syncwarp();
 
     // Pilot search (search.comp:126-175), next bucket's keys prefetched.
     const FastMod fm = FastMod::make(ps ? ps : 1);
     uint32_t k_lim = 0x80000000u / (ps ? ps : 1);
     if (k_lim > a.k_max) k_lim = a.k_max;
     uint32_t sc_next = nonempty ? ws.sched[0] : 0u;
-    uint2 L_next = lane < (int)(sc_next >> 16) ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
+    uint32_t s_next = nonempty ? half_get(ws.cnt32, sc_next >> 16) : 0u;
+    uint2 L_next = lane < (int)s_next ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
     for (uint32_t j = 0; j < nonempty; j++) {
-        const uint32_t sc = sc_next;
+        const uint32_t sc = sc_next, s = s_next;
         const uint2 L = L_next;
-        const uint32_t b = ws.order[j];
-        const uint32_t s = sc >> 16, st = sc & 0xFFFFu;
+        const uint32_t b = sc >> 16, st = sc & 0xFFFFu;
         if (j + 1 < nonempty) {
             sc_next = ws.sched[j + 1];
-            L_next = lane < (int)(sc_next >> 16) ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
+            s_next = half_get(ws.cnt32, sc_next >> 16);
+            L_next = lane < (int)s_next ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
         }
         uint32_t pilot = 0;
         const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, lane, &pilot)
@@ -375,7 +373,7 @@ int search_warps_per_cta(uint32_t buckets, uint32_t cap) {
     return (int)(fit < (size_t)kSearchWarps ? fit : (size_t)kSearchWarps);
 }
 
-__global__ void __launch_bounds__(kSearchWarps * 32, 4) k_search(SearchArgs a) {
+__global__ void __launch_bounds__(kSearchWarps * 32, kSearchCtasPerSm) k_search(SearchArgs a) {
     extern __shared__ __align__(16) uint32_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const WarpSmem ws = carve(smem + (size_t)warp * warp_words(a.buckets, a.cap), a.buckets, a.cap);
