@@ -30,8 +30,10 @@
 // window is (h >> 5) + (w >> 5) and its bit shift is h & 31 for every lane.
 //
 // Buckets of at most 32 keys (nearly all of them) keep one key per lane in
-// registers, test collisions with __match_any_sync and broadcast slots with
-// shuffles; larger buckets stage keys and slots in shared memory.
+// registers and test collisions with __match_any_sync; for at most 8 keys the
+// offset search also keeps every slot in registers, for 9..32 keys it reads them
+// from shared memory four at a time.  Larger buckets read their keys from the
+// bucket-ordered copy in global memory and stage their slots in shared memory.
 #include "kernels.cuh"
 
 namespace phobicb200 {
@@ -166,6 +168,46 @@ __device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, const
     return kNone;
 }
 
+// The same search for a bucket of at most K <= 8 keys, with the packed slots in
+// registers: hp is this lane's packed slot, lanes >= the bucket size hold slot 0's.
+// Each key's bitmap address is formed once per call (occ + (h >> 5) words); a round
+// adds the lane's window offset.  K == 8 tests the second half only when some live
+// window is still open after the first four keys.  Dead lanes (w >= ps) read at
+// offset 0, inside the bitmap, and count as fully occupied.
+template <int K>
+__device__ __forceinline__ uint32_t first_free_offset_reg(const uint32_t *occ, uint32_t hp, uint32_t ps, int lane) {
+    const uint32_t occ_sa = (uint32_t)__cvta_generic_to_shared(occ);
+    uint32_t v[K], hb[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        v[i] = __shfl_sync(kFullMask, hp, i);
+        hb[i] = occ_sa + (v[i] >> 5);
+    }
+    for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
+        const uint32_t w = w0 + 32 * lane;
+        const bool live = w < ps;
+        const uint32_t lo = live ? (w >> 3) : 0u;
+        uint32_t bad = 0;
+#pragma unroll
+        for (int i = 0; i < (K < 4 ? K : 4); i++) bad |= __funnelshift_r(lds32(hb[i] + lo), lds32_next(hb[i] + lo), v[i]);
+        if (K == 8) {
+            if (!__all_sync(kFullMask, bad == kFullMask || !live)) {
+#pragma unroll
+                for (int i = 4; i < K; i++)
+                    bad |= __funnelshift_r(lds32(hb[i] + lo), lds32_next(hb[i] + lo), v[i]);
+            }
+        }
+        uint32_t valid = live ? ~bad : 0u;
+        if (live && ps - w < 32) valid &= (1u << (ps - w)) - 1u;
+        const uint32_t ball = __ballot_sync(kFullMask, valid != 0);
+        if (ball) {
+            const int f = __ffs(ball) - 1;
+            return w0 + 32 * f + __ffs(__shfl_sync(kFullMask, valid, f)) - 1;
+        }
+    }
+    return kNone;
+}
+
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
 __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
                                                 uint32_t k_lim, int lane, uint32_t *pilot) {
@@ -186,10 +228,17 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
             if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
         }
         const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
-        if (lane < (int)padded) ws.hs[lane] = hp;
-        __syncwarp();
-        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
-        __syncwarp();
+        uint32_t o;
+        if (s == 1) o = first_free_offset_reg<1>(ws.occ, hp, ps, lane);
+        else if (s == 2) o = first_free_offset_reg<2>(ws.occ, hp, ps, lane);
+        else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane);
+        else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane);
+        else {
+            if (lane < (int)padded) ws.hs[lane] = hp;
+            __syncwarp();
+            o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+            __syncwarp();
+        }
         if (o == kNone) continue;
         if (mine) {
             uint32_t q = h + o;
