@@ -49,6 +49,14 @@ __host__ __device__ __forceinline__ uint32_t occ_words(uint32_t cap) { return (2
 // Collision scratch of large buckets: one bit per slot.
 __host__ __device__ __forceinline__ uint32_t scr_words(uint32_t cap) { return (cap + 31) / 32 + 1; }
 __host__ __device__ __forceinline__ uint32_t half_words(uint32_t B) { return (B + 1) / 2; }
+// Words of the bitmap: the doubled bitmap plus room for every read of the
+// register-path offset search, which reads, for a slot h < ps and lane L in round
+// r < ceil(ps / 1024), words (h >> 5) + L + 32 r and the one after it, dead lanes
+// included; the bound covers it for every ps <= cap.
+__host__ __device__ __forceinline__ uint32_t bitmap_words(uint32_t cap) {
+    uint32_t reach = (cap - 1) / 32 + 32 * ((cap + 1023) / 1024) + 2;
+    return reach > occ_words(cap) ? reach : occ_words(cap);
+}
 
 // Per-warp shared memory, in 32-bit words.  Every warp's region starts on a
 // 16-byte boundary (its size is rounded up to 4 words) and the union comes
@@ -65,7 +73,7 @@ __host__ __device__ __forceinline__ size_t union_words(uint32_t B, uint32_t cap)
 }
 
 __host__ __device__ __forceinline__ size_t warp_words(uint32_t B, uint32_t cap) {
-    size_t w = union_words(B, cap) + half_words(B) + (size_t)B + (size_t)occ_words(cap);
+    size_t w = union_words(B, cap) + half_words(B) + (size_t)B + (size_t)bitmap_words(cap);
     return (w + 3) & ~size_t(3);
 }
 
@@ -208,9 +216,63 @@ __device__ __forceinline__ uint32_t first_free_offset_reg(const uint32_t *occ, u
     return kNone;
 }
 
+template <int OFF>
+__device__ __forceinline__ uint32_t lds32_at(uint32_t addr) {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1+%2];" : "=r"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+
+// Round R (offsets [1024 R, 1024 R + 1024)) of first_free_offset_unr: true when
+// some lane's window holds a free offset, which is written to *o.
+template <int K, int R>
+__device__ __forceinline__ bool scan_round(const uint32_t (&hb)[K], const uint32_t (&v)[K], uint32_t ps, int lane,
+                                           uint32_t *o) {
+    // Offsets of this lane's window below ps, as a mask (clamped funnel shift: n >= 32 gives all ones).
+    const int n = (int)ps - (int)(1024 * R) - 32 * lane;
+    uint32_t bad = ~__funnelshift_lc(kFullMask, 0u, (uint32_t)max(n, 0));
+#pragma unroll
+    for (int i = 0; i < (K < 4 ? K : 4); i++)
+        bad |= __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i]);
+    if (K == 8) {
+        if (!__all_sync(kFullMask, bad == kFullMask)) {
+#pragma unroll
+            for (int i = 4; i < K; i++)
+                bad |= __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i]);
+        }
+    }
+    const uint32_t ball = __ballot_sync(kFullMask, bad != kFullMask);
+    if (!ball) return false;
+    const int f = __ffs(ball) - 1;
+    *o = 1024u * R + 32u * f + __ffs(~__shfl_sync(kFullMask, bad, f)) - 1;
+    return true;
+}
+
+// first_free_offset_reg for ps <= 4096: the (at most four) rounds unrolled, each
+// key's window address formed once per call with the lane's word offset included,
+// so a round reads at a constant 128 R bytes further.  Dead lanes (offsets >= ps)
+// read inside the padded bitmap (bitmap_words) and are masked.
+template <int K>
+__device__ __forceinline__ uint32_t first_free_offset_unr(const uint32_t *occ, uint32_t hp, uint32_t ps,
+                                                          uint32_t rounds, int lane) {
+    const uint32_t lane_sa = (uint32_t)__cvta_generic_to_shared(occ) + 4u * lane;
+    uint32_t v[K], hb[K];
+#pragma unroll
+    for (int i = 0; i < K; i++) {
+        v[i] = __shfl_sync(kFullMask, hp, i);
+        hb[i] = lane_sa + (v[i] >> 5);
+    }
+    uint32_t o = kNone;
+    if (scan_round<K, 0>(hb, v, ps, lane, &o)) return o;
+    if (rounds > 1 && scan_round<K, 1>(hb, v, ps, lane, &o)) return o;
+    if (rounds > 2 && scan_round<K, 2>(hb, v, ps, lane, &o)) return o;
+    if (rounds > 3 && scan_round<K, 3>(hb, v, ps, lane, &o)) return o;
+    return kNone;
+}
+
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
 __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
-                                                uint32_t k_lim, int lane, uint32_t *pilot) {
+                                                uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
     const bool mine = lane < (int)s;
     const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
@@ -229,7 +291,12 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
         }
         const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
         uint32_t o;
-        if (s == 1) o = first_free_offset_reg<1>(ws.occ, hp, ps, lane);
+        if (s <= 8 && rounds <= 4) {
+            if (s == 1) o = first_free_offset_unr<1>(ws.occ, hp, ps, rounds, lane);
+            else if (s == 2) o = first_free_offset_unr<2>(ws.occ, hp, ps, rounds, lane);
+            else if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane);
+            else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane);
+        } else if (s == 1) o = first_free_offset_reg<1>(ws.occ, hp, ps, lane);
         else if (s == 2) o = first_free_offset_reg<2>(ws.occ, hp, ps, lane);
         else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane);
         else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane);
@@ -300,7 +367,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     const uint32_t base = a.G[(size_t)g * a.gstride];
     const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
     if (ps > a.cap) return PHOBIC_OK;  // reported by the size check
-    const uint32_t ow = occ_words(a.cap);
+    const uint32_t ow = bitmap_words(a.cap);
     uint32_t *pil = d.pilots + p;
     const size_t pstride = d.partitions;
 
@@ -389,6 +456,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
 
     // Pilot search (search.comp:126-175), next bucket's keys prefetched.
     const FastMod fm = FastMod::make(ps ? ps : 1);
+    const uint32_t rounds = (ps + 1023) / 1024;
     uint32_t k_lim = 0x80000000u / (ps ? ps : 1);
     if (k_lim > a.k_max) k_lim = a.k_max;
     uint32_t sc_next = nonempty ? ws.sched[0] : 0u;
@@ -404,7 +472,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
             L_next = lane < (int)s_next ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
         }
         uint32_t pilot = 0;
-        const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, lane, &pilot)
+        const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
                                          : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
         if (st_code != PHOBIC_OK) return st_code;
         if (lane == 0) pil[(size_t)b * pstride] = pilot;
