@@ -332,16 +332,23 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
             }
             if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
         }
-        bool d = false;
-        for (uint32_t i = lane; i < s; i += 32) {
-            uint2 key = src[i];
-            uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
-            ws.hs[i] = pack_slot(h);
-            uint32_t bit = 1u << (h & 31);
-            d |= (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+        // Hash chunk by chunk; stop at the first chunk that repeats a slot.
+        bool dup = false;
+        uint32_t done = 0;  // keys hashed (and marked in the collision scratch)
+        for (uint32_t c0 = 0; c0 < s && !dup; c0 += 32) {
+            const uint32_t i = c0 + lane;
+            bool d = false;
+            if (i < s) {
+                const uint2 key = src[i];
+                const uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
+                ws.hs[i] = pack_slot(h);
+                const uint32_t bit = 1u << (h & 31);
+                d = (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+            }
+            dup = __any_sync(kFullMask, d);
+            done = c0 + 32;
         }
-        const bool dup = __any_sync(kFullMask, d);
-        for (uint32_t i = lane; i < s; i += 32) ws.scr[unpack_slot(ws.hs[i]) >> 5] = 0;
+        for (uint32_t i = lane; i < s && i < done; i += 32) ws.scr[unpack_slot(ws.hs[i]) >> 5] = 0;
         __syncwarp();
         if (dup) continue;
         if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
@@ -352,6 +359,76 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
         for (uint32_t i = lane; i < s; i += 32) {
             uint32_t q = unpack_slot(ws.hs[i]) + o;
             mark(ws.occ, q >= ps ? q - ps : q, ps);
+        }
+        __syncwarp();
+        *pilot = o + ps * k;
+        return PHOBIC_OK;
+    }
+    return PHOBIC_ERR_SEARCH_LIMIT;
+}
+
+// place_large with the bucket's keys in registers: key i = 32 c + lane in key[c],
+// loaded once per bucket (C chunks of 32, 32 C >= s).  Each try hashes chunk by
+// chunk and stops at the first chunk that repeats a slot, so a bucket that
+// collides (the large ones of a partition collide often) hashes about half its
+// keys per rejected counter.  Slots go to ws.hs for the offset search and the
+// marking, as in place_large.
+template <int C>
+__device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const uint2 *src, uint32_t s, uint32_t ps,
+                                                    FastMod fm, uint32_t k_lim, int lane, uint32_t *pilot) {
+    const uint32_t padded = (s + 3) & ~3u;
+    uint2 key[C];
+#pragma unroll
+    for (int c = 0; c < C; c++) key[c] = 32 * c + lane < (int)s ? src[32 * c + lane] : make_uint2(0, 0);
+    for (uint32_t k = 0; k < k_lim; k++) {
+        if (k == kDupCheckAt) {
+            bool d = false;
+            for (uint32_t t = 0; t + 1 < s; t++) {
+                uint2 kt = src[t];
+#pragma unroll
+                for (int c = 0; c < C; c++) {
+                    const uint32_t i = 32 * c + lane;
+                    d |= i > t && i < s && key[c].x == kt.x && key[c].y == kt.y;
+                }
+            }
+            if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
+        }
+        bool dup = false;
+        int done = 0;  // chunks hashed (and marked in the collision scratch)
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            if (!dup && 32 * c < (int)s) {
+                const uint32_t i = 32 * c + lane;
+                bool d = false;
+                if (i < s) {
+                    const uint32_t h = fm.mod(pilot_hash(key[c].x, key[c].y, k));
+                    ws.hs[i] = pack_slot(h);
+                    const uint32_t bit = 1u << (h & 31);
+                    d = (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+                }
+                dup = __any_sync(kFullMask, d);
+                done = c + 1;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const uint32_t i = 32 * c + lane;
+            if (c < done && i < s) ws.scr[unpack_slot(ws.hs[i]) >> 5] = 0;
+        }
+        __syncwarp();
+        if (dup) continue;
+        if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
+        __syncwarp();
+        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+        __syncwarp();
+        if (o == kNone) continue;
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const uint32_t i = 32 * c + lane;
+            if (i < s) {
+                uint32_t q = unpack_slot(ws.hs[i]) + o;
+                mark(ws.occ, q >= ps ? q - ps : q, ps);
+            }
         }
         __syncwarp();
         *pilot = o + ps * k;
@@ -473,7 +550,8 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         }
         uint32_t pilot = 0;
         const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
-                                         : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
+                                 : s <= 64  ? place_large_reg<2>(ws, so + st, s, ps, fm, k_lim, lane, &pilot)
+                                            : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
         if (st_code != PHOBIC_OK) return st_code;
         if (lane == 0) pil[(size_t)b * pstride] = pilot;
     }
