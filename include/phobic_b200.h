@@ -173,6 +173,29 @@ PHOBIC_API phobic_status phobic_encode(int pilot_encoder, int offset_encoder, co
                                        const phobic_params *params, float tradeoff, uint8_t *out, size_t cap,
                                        size_t *size, double *bits_per_key);
 
+/* Mphf::setData on the GPU for the encoders made of compact vectors: pilot_encoder
+ * 0 (interleaved<compact>) or 3 (mono<compact>), offset_encoder 0 (diff_partition
+ * <compact>) or 1 (direct_partition<compact>); other encoders are PHOBIC_ERR_INVALID
+ * (use phobic_encode).  Same bytes, in the same visit order, and the same
+ * bits_per_key as phobic_encode for these encoders (interleaved_encoder.hpp:8-15,
+ * mono_encoders.hpp, linear_diff_encoder.hpp:15-28, compact_vector.hpp).
+ * built's arrays are read on the device when built->on_device, else copied in.
+ * out (host memory, or device memory when out_on_device) receives at most cap
+ * bytes and may be NULL; *size = the full byte count.  Synchronous. */
+PHOBIC_API phobic_status phobic_encode_gpu(phobic_ctx *ctx, int pilot_encoder, int offset_encoder,
+                                           const phobic_result *built, uint32_t partitions,
+                                           const phobic_params *params, uint8_t *out, size_t cap,
+                                           int out_on_device, size_t *size, double *bits_per_key);
+
+/* Device arrays owned by the context for one build result of `partitions`
+ * partitions (pilots [buckets * partitions], offsets [partitions + 1]), so that a
+ * caller without its own device memory can build into the device and encode from
+ * there (phobic_build with *out, then phobic_encode_gpu).  *out->on_device = 1.
+ * The arrays stay valid until the next call of this function on the context or
+ * its destruction. */
+PHOBIC_API phobic_status phobic_ctx_result(phobic_ctx *ctx, uint32_t buckets, uint32_t partitions,
+                                           phobic_result *out);
+
 /* ------------------------------------------------------------------ query
  * MPHF::operator() (mphf.hpp:77-86) over the raw (unencoded) result arrays.
  * positions[i] = slot of key i in [0, n_built).  Arrays may live on the host

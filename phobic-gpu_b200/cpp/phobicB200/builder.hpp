@@ -5,7 +5,9 @@
 // for keyType in {uint64_t, std::string, std::pair<uint64_t,uint64_t>, Key}.  The host
 // hash, the Vulkan runtime and the seven compute stages are replaced by one call to
 // phobic_build, which hashes on the device and returns the pilots and partition
-// offsets that Mphf::setData encodes.  Link with -lphobic_b200.
+// offsets that Mphf::setData encodes.  For the compact-vector encoders the result
+// stays on the device and phobic_encode_gpu writes the encoders' bytes, which the
+// MPHF loads.  Link with -lphobic_b200.
 #pragma once
 
 #include <chrono>
@@ -18,6 +20,7 @@
 #include <vector>
 
 #include "config.hpp"
+#include "encoders.hpp"
 #include "phobic_b200.h"
 
 namespace phobicgpu {
@@ -98,25 +101,51 @@ class MPHFbuilder {
         }
         timer.addLabel("input_pack");
         const uint32_t partitions = phobic_partitions(keys.size(), config_.partitionSize);
+        constexpr int pe = gpu_pilot_code<typename Mphf::pilot_encoder_type>::value;
+        constexpr int oe = gpu_offset_code<typename Mphf::offset_encoder_type>::value;
+        if constexpr (pe >= 0 && oe >= 0) {
+            // Compact-vector encoders: the result stays on the device and is encoded
+            // there; only the encoded bytes come back.
+            phobic_result r{};
+            phobic_timings t{};
+            check(phobic_ctx_result(ctx_, config_.bucketCountPerPartition, partitions, &r));
+            check(phobic_build(ctx_, &k, &params, &r, &t));
+            timer.addLabel("gpu_build");
+            add_gpu_labels(timer, t);
+            size_t size = 0;
+            check(phobic_encode_gpu(ctx_, pe, oe, &r, partitions, &params, nullptr, 0, 0, &size, nullptr));
+            std::vector<uint8_t> encoded(size);
+            check(phobic_encode_gpu(ctx_, pe, oe, &r, partitions, &params, encoded.data(), size, 0, &size, nullptr));
+            if (!f.loadEncoded(encoded.data(), size, partitions, config_))
+                throw std::runtime_error("phobic: encoded bytes do not match the MPHF's encoders");
+            timer.addLabel("encoding");
+            return timer;
+        }
         std::vector<uint32_t> pilots((size_t)partitions * config_.bucketCountPerPartition);
         std::vector<uint32_t> part_off(partitions + 1);
         phobic_result r{0, pilots.data(), part_off.data()};
         phobic_timings t{};
-        phobic_status s = phobic_build(ctx_, &k, &params, &r, &t);
-        if (s != PHOBIC_OK) throw std::runtime_error(std::string("phobic: ") + phobic_last_error(ctx_));
+        check(phobic_build(ctx_, &k, &params, &r, &t));
         timer.addLabel("gpu_build");
-        timer.addLabelManually("GPU_input_transfer", t.input_transfer);
-        timer.addLabelManually("GPU_bucket_sizes", t.bucket_sizes);
-        timer.addLabelManually("GPU_partition_offsets", t.partition_offsets);
-        timer.addLabelManually("GPU_key_redistribution", t.key_redistribution);
-        timer.addLabelManually("GPU_search", t.search);
-        timer.addLabelManually("GPU_result_transfer", t.result_transfer);
+        add_gpu_labels(timer, t);
         f.setData(pilots, part_off, partitions, config_);
         timer.addLabel("encoding");
         return timer;
     }
 
   private:
+    void check(phobic_status s) const {
+        if (s != PHOBIC_OK) throw std::runtime_error(std::string("phobic: ") + phobic_last_error(ctx_));
+    }
+    static void add_gpu_labels(HostTimer &timer, const phobic_timings &t) {
+        timer.addLabelManually("GPU_input_transfer", t.input_transfer);
+        timer.addLabelManually("GPU_bucket_sizes", t.bucket_sizes);
+        timer.addLabelManually("GPU_partition_offsets", t.partition_offsets);
+        timer.addLabelManually("GPU_key_redistribution", t.key_redistribution);
+        timer.addLabelManually("GPU_search", t.search);
+        timer.addLabelManually("GPU_result_transfer", t.result_transfer);
+    }
+
     MPHFconfig config_;
     phobic_ctx *ctx_ = nullptr;
 };

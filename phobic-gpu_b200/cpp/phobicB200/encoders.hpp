@@ -154,6 +154,8 @@ struct interleaved_encoder {
         for (int64_t j = 0; j < (int64_t)buckets; j++) encoders[j].encode(begin + j * partitions, partitions);
     }
     uint64_t access(uint64_t partition, uint64_t bucket) const { return encoders[bucket].access(partition); }
+    // Shape for loading from serialised bytes (the bytes do not hold the column count).
+    void set_shape(uint64_t, uint64_t buckets) { encoders.assign(buckets, BaseEncoder()); }
     std::string name() { return "InterEncoder<" + BaseEncoder::name() + ">"; }
     uint64_t num_bits() const {
         uint64_t s = 0;
@@ -215,6 +217,7 @@ struct mono_encoder {
     size_t size() const { return enc.size(); }
     size_t num_bits() const { return enc.num_bits(); }
     uint64_t access(uint64_t partition, uint64_t bucket) const { return enc.access(partitions * bucket + partition); }
+    void set_shape(uint64_t partitions_, uint64_t) { partitions = partitions_; }
     template <typename Visitor>
     void visit(Visitor &visitor) { visitor.visit(enc); }
 
@@ -246,6 +249,7 @@ struct linear_diff_encoder {
     static std::string name() { return BaseEncoder::name(); }
     size_t size() const { return enc.size(); }
     size_t num_bits() const { return enc.num_bits(); }
+    void set_increment(uint64_t inc) { increment = int64_t(inc); }
     uint64_t access(uint64_t i) const {
         const uint64_t c = enc.access(i);
         const int64_t d = (int64_t(c & 1) * 2 - 1) * int64_t(c >> 1);
@@ -264,6 +268,7 @@ struct diff_partition_encoder {
     template <typename Iterator>
     void encode(Iterator begin, uint64_t partition_size, uint64_t count) { enc.encode(begin, count, partition_size); }
     static std::string name() { return "DiffToExpected<" + BaseEncoder::name() + ">"; }
+    void set_shape(uint64_t partition_size) { enc.set_increment(partition_size); }
     size_t size() const { return enc.size(); }
     size_t num_bits() const { return enc.num_bits(); }
     uint64_t access(uint64_t partition) const { return enc.access(partition); }
@@ -279,6 +284,7 @@ struct direct_partition_encoder {
     template <typename Iterator>
     void encode(Iterator begin, uint64_t, uint64_t count) { enc.encode(begin, count); }
     static std::string name() { return "Direct<" + BaseEncoder::name() + ">"; }
+    void set_shape(uint64_t) {}
     size_t size() const { return enc.size(); }
     size_t num_bits() const { return enc.num_bits(); }
     uint64_t access(uint64_t partition) const { return enc.access(partition); }
@@ -288,5 +294,20 @@ struct direct_partition_encoder {
   private:
     BaseEncoder enc;
 };
+
+// Encoder codes of phobic_encode / phobic_encode_gpu for the encoders whose bytes
+// the GPU writes (compact-vector encoders); -1 for the others.
+template <typename E>
+struct gpu_pilot_code { static constexpr int value = -1; };
+template <>
+struct gpu_pilot_code<interleaved_encoder<compact>> { static constexpr int value = 0; };
+template <>
+struct gpu_pilot_code<mono_encoder<compact>> { static constexpr int value = 3; };
+template <typename E>
+struct gpu_offset_code { static constexpr int value = -1; };
+template <>
+struct gpu_offset_code<diff_partition_encoder<compact>> { static constexpr int value = 0; };
+template <>
+struct gpu_offset_code<direct_partition_encoder<compact>> { static constexpr int value = 1; };
 
 }  // namespace phobicgpu

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -10,6 +11,47 @@
 #include "encoders.hpp"
 
 namespace phobicgpu {
+
+// Reads serialised fields in visit order: a trivially copyable value as its bytes,
+// a vector as its size_t count followed by its elements.
+struct ByteLoader {
+    const uint8_t *bytes;
+    size_t size;
+    size_t pos = 0;
+    bool ok = true;
+
+    void get(void *dst, size_t n) {
+        if (!ok || n > size - pos) {
+            ok = false;
+            std::memset(dst, 0, n);
+            return;
+        }
+        std::memcpy(dst, bytes + pos, n);
+        pos += n;
+    }
+    template <typename T>
+    void visit(std::vector<T> &v) {
+        size_t n = 0;
+        get(&n, sizeof(n));
+        if (!ok) return;
+        if constexpr (std::is_trivially_copyable_v<T>) {
+            if (n > (size - pos) / sizeof(T)) {
+                ok = false;
+                return;
+            }
+            v.resize(n);
+            if (n) get(v.data(), n * sizeof(T));
+        } else {
+            v.resize(n);
+            for (auto &e : v) visit(e);
+        }
+    }
+    template <typename T>
+    void visit(T &v) {
+        if constexpr (std::is_trivially_copyable_v<T>) get(&v, sizeof(T));
+        else v.visit(*this);
+    }
+};
 
 template <typename PilotEncoder, typename PartitionOffsetEncoder, typename Hasher>
 class MPHF {
@@ -23,6 +65,9 @@ class MPHF {
     uint64_t getBucket(uint32_t bucketer) const { return phobicb200::bucket_of_query(bucketer, fulcs.data()); }
 
   public:
+    using pilot_encoder_type = PilotEncoder;
+    using offset_encoder_type = PartitionOffsetEncoder;
+
     PilotEncoder &getPilotEncoder() { return pilots; }
     PartitionOffsetEncoder &getPartitionOffsetEncoder() { return partitionOffsets; }
     uint32_t getPartitions() const { return partitions; }
@@ -42,6 +87,21 @@ class MPHF {
         partitions = parts;
         partitionOffsets.encode(offsets.begin(), config.partitionSize, parts + 1);
         pilots.encode(pilot_values.begin(), parts, config.bucketCountPerPartition);  // columns in parallel
+    }
+
+    // The state setData produces, read back from the encoders' serialised bytes
+    // (pilot encoder, then partition-offset encoder, in visit order, as
+    // phobic_encode and phobic_encode_gpu write them).  False when the bytes do
+    // not hold exactly the two encoders.
+    bool loadEncoded(const uint8_t *bytes, size_t size, uint32_t parts, const MPHFconfig &config) {
+        fulcs = config.getFulcs();
+        partitions = parts;
+        pilots.set_shape(parts, config.bucketCountPerPartition);
+        partitionOffsets.set_shape(config.partitionSize);
+        ByteLoader loader{bytes, size};
+        pilots.visit(loader);
+        partitionOffsets.visit(loader);
+        return loader.ok && loader.pos == size;
     }
 
     // Slot of a key in [0, n) (mphf.hpp:77-86).

@@ -13,6 +13,8 @@ using namespace phobicb200;
 struct phobic_ctx {
     Worker w;
     std::string last_error;
+    DeviceArena results;  // phobic_ctx_result
+    DeviceArena encoded;  // phobic_encode_gpu output staging
 };
 
 extern "C" {
@@ -223,6 +225,29 @@ phobic_status phobic_query(phobic_ctx *ctx, const phobic_keys *keys, const phobi
     if (!ctx) return PHOBIC_ERR_INVALID;
     ctx->last_error.clear();
     return run_query(ctx->w, keys, params, partitions, built, positions, nullptr, &ctx->last_error);
+}
+
+phobic_status phobic_encode_gpu(phobic_ctx *ctx, int pilot_encoder, int offset_encoder, const phobic_result *built,
+                                uint32_t partitions, const phobic_params *params, uint8_t *out, size_t cap,
+                                int out_on_device, size_t *size, double *bits_per_key) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return run_encode_gpu(ctx->w, ctx->encoded, pilot_encoder, offset_encoder, built, partitions, params, out, cap,
+                          out_on_device, size, bits_per_key, &ctx->last_error);
+}
+
+phobic_status phobic_ctx_result(phobic_ctx *ctx, uint32_t buckets, uint32_t partitions, phobic_result *out) {
+    if (!ctx || !out || buckets == 0) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    const size_t pb = align256(4 * (size_t)buckets * partitions), ob = align256(4 * ((size_t)partitions + 1));
+    cudaError_t e = cudaSetDevice(ctx->w.device);
+    if (e == cudaSuccess) e = ctx->results.reserve(pb + ob);
+    if (e != cudaSuccess) return cuda_status(e, "phobic_ctx_result", &ctx->last_error);
+    ctx->results.reset();
+    out->on_device = 1;
+    out->pilots = static_cast<uint32_t *>(ctx->results.take(pb));
+    out->partition_offsets = static_cast<uint32_t *>(ctx->results.take(ob));
+    return PHOBIC_OK;
 }
 
 phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,

@@ -86,11 +86,6 @@ phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
     return PHOBIC_ERR_CUDA;
 }
 
-#define PHB_TRY(expr, what)                                  \
-    do {                                                     \
-        phobic_status s_ = cuda_status((expr), (what), err); \
-        if (s_ != PHOBIC_OK) return s_;                      \
-    } while (0)
 
 phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) {
     auto t0 = std::chrono::steady_clock::now();

@@ -88,6 +88,22 @@ phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err);
 
 phobic_status cuda_status(cudaError_t e, const char *what, std::string *err);
 
+// Returns the status of a failed CUDA call from the enclosing function (which has
+// a std::string *err).
+#define PHB_TRY(expr, what)                                  \
+    do {                                                     \
+        phobic_status s_ = cuda_status((expr), (what), err); \
+        if (s_ != PHOBIC_OK) return s_;                      \
+    } while (0)
+
+// Encoding of a build's result on the device (compact-vector encoders; see
+// phobic_encode_gpu).  out_arena holds the packed bytes when they cannot be
+// written to `out` directly.
+phobic_status run_encode_gpu(Worker &w, DeviceArena &out_arena, int pilot_encoder, int offset_encoder,
+                             const phobic_result *built, uint32_t partitions, const phobic_params *params,
+                             uint8_t *out, size_t cap, int out_on_device, size_t *size, double *bits_per_key,
+                             std::string *err);
+
 // Query / verification over raw build output.
 phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params *params, uint32_t partitions,
                         const phobic_result *built, uint32_t *positions, uint64_t *bad, std::string *err);

@@ -137,6 +137,9 @@ def _lib() -> C.CDLL:
         "phobic_debug_stalled_wait": (I32, [P, U32, C.POINTER(I32)]),
         "phobic_encode": (I32, [I32, I32, P, P, U32, C.POINTER(Params), C.c_float, P, C.c_size_t,
                                 C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
+        "phobic_encode_gpu": (I32, [P, I32, I32, C.POINTER(Result), U32, C.POINTER(Params), P, C.c_size_t, I32,
+                                    C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
+        "phobic_ctx_result": (I32, [P, U32, U32, C.POINTER(Result)]),
         "phobic_build_noalloc": (I32, [C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P]),
         "phobic_server_create": (I32, [C.POINTER(ServerConfig), PP]),
         "phobic_server_submit": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
@@ -387,6 +390,26 @@ def encode(built: BuildResult, cfg: MPHFconfig, pilot_encoder: str = "interleave
     buf = np.zeros(size.value, np.uint8)
     check(_lib().phobic_encode(*args, buf.ctypes.data, size.value, C.byref(size), C.byref(bpk)))
     return buf.tobytes(), bpk.value
+
+
+def encode_gpu(ctx: "Context", built: BuildResult, cfg: MPHFconfig, pilot_encoder: str = "interleaved_compact",
+               offset_encoder: str = "diff", out=None) -> tuple[bytes | None, float, int]:
+    """Mphf::setData on the GPU for the compact-vector encoders (interleaved_compact or
+    mono_compact pilots, diff or direct offsets): (serialised bytes, bits per key, size).
+    The bytes equal encode()'s.  built's arrays may be torch CUDA tensors (read in
+    place) or numpy arrays.  With out (a torch CUDA uint8 tensor) the bytes are
+    written there and None is returned in their place."""
+    res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
+    size, bpk = C.c_size_t(), C.c_double()
+    args = (ctx.handle, PILOT_ENCODERS[pilot_encoder], OFFSET_ENCODERS[offset_encoder], C.byref(res),
+            built.partitions, C.byref(cfg.params))
+    if out is not None:
+        check(_lib().phobic_encode_gpu(*args, _ptr(out), out.numel(), 1, C.byref(size), C.byref(bpk)), ctx)
+        return None, bpk.value, size.value
+    check(_lib().phobic_encode_gpu(*args, None, 0, 0, C.byref(size), C.byref(bpk)), ctx)
+    buf = np.zeros(max(size.value, 1), np.uint8)
+    check(_lib().phobic_encode_gpu(*args, buf.ctypes.data, size.value, 0, C.byref(size), C.byref(bpk)), ctx)
+    return buf[: size.value].tobytes(), bpk.value, size.value
 
 
 # ------------------------------------------------------------------ batch and serving
