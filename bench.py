@@ -265,6 +265,22 @@ def run_ours(args) -> None:
     if tp.exists():
         tr = json.loads(tp.read_text())
         traffic = tr.get("bytes_per_key", 0) * n if tr.get("bytes_per_key") else None
+    # Issue-rate view of K4 (it is bound by instruction issue, not HBM): warp
+    # instructions per launch from the ncu capture of the same kernel (per partition,
+    # scaled by partitions) over the K4 event time, against 4 schedulers per SM at the
+    # SM clock sampled during the timed region.
+    issue = None
+    ip = ROOT / "profiles" / "k4_issue.json"
+    clk = clocks.summary()
+    if ip.exists() and clk.get("sm_mhz"):
+        per_part = json.loads(ip.read_text())["warp_instructions_per_partition"]
+        sms = torch.cuda.get_device_properties(local).multi_processor_count
+        inst = per_part * parts
+        ach = inst / (k4_ms / 1e3)
+        peak_issue = sms * 4 * clk["sm_mhz"] * 1e6
+        issue = {"warp_inst_per_launch": inst, "achieved": ach, "peak": peak_issue, "unit": "warp-inst/s",
+                 "frac": ach / peak_issue, "sm_count": sms, "sm_mhz": clk["sm_mhz"],
+                 "source": "profiles/k4_issue.json (ncu smsp__inst_executed per partition x partitions)"}
     base = cpu_baseline(args.cpu_sample) if not args.no_cpu_baseline else None
     line = {
         "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world, "steps": args.steps,
@@ -283,7 +299,7 @@ def run_ours(args) -> None:
         "roofline": {"kernel": "k_search (K4)", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "bytes_per_key": K4_BYTES_PER_KEY,
-                     "launch_ms": k4_ms},
+                     "launch_ms": k4_ms, "issue": issue},
         "encoding": {"encoder": "interleaved<dictionary> + diff<compact>", "ms": encode_ms,
                      "bits_per_key": bits_per_key, "bytes": len(blob), "host_threads": os.cpu_count(),
                      "e2e_with_encoding_mkeys_s": world * n / ((e2e_ms + encode_ms) / 1e3) / 1e6},
@@ -293,7 +309,7 @@ def run_ours(args) -> None:
                              "note": "gpu_ms: phobic_encode_gpu from the device-resident result, bytes copied to "
                                      "host memory (wall clock, best of 3)"},
         "cpu_baseline": base,
-        "clocks": clocks.summary(),
+        "clocks": clk,
     }
     print(json.dumps(line), flush=True)
     ctx.close()
