@@ -12,7 +12,9 @@
 // so an MPHF serialised with visit() has the same bytes as the reference's.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <unordered_map>
 #include <utility>
@@ -53,32 +55,151 @@ struct rice {
 };
 
 // Dictionary codes: every distinct value gets a rank by non-increasing frequency
-// (encoders.hpp:145-177).  Ranks of equal frequency depend on the standard
-// library's hash-table iteration order and on std::sort; the same standard
-// library reproduces the reference's bytes.
+// (encoders.hpp:145-177).  Ranks of equal frequency follow the standard library's
+// hash-table iteration order and std::sort, as in the reference.
+//
+// The reference counts with find/insert on a std::unordered_map for every value
+// and looks every value up again for its rank.  Here the counting and the rank
+// lookups use a flat open-addressing table, and the std::unordered_map only
+// receives the distinct values, in first-occurrence order, with operator[]: the
+// reference's map changes only when a value is first seen, so the same insertions
+// in the same order give the same buckets, the same node order and therefore the
+// same iteration order (node memory comes from a per-call arena, which the order
+// does not depend on).  std::sort then sees the same sequence and returns the
+// same permutation, so the bytes are the reference's.
 namespace dict_detail {
+
+// Value -> u64 slot value; open addressing with linear probing, grown at half load.
+class FlatMap {
+  public:
+    explicit FlatMap(size_t expect) {
+        int lg = 4;
+        while ((size_t(1) << lg) < 2 * expect && lg < 40) lg++;
+        init(lg);
+    }
+    // Slot of v, inserted with value 0 when absent (*fresh says which).  A slot
+    // index is valid until the next insertion.
+    size_t find_or_insert(uint64_t v, bool *fresh) {
+        if (2 * (used_ + 1) > keys_.size()) grow();
+        size_t h = home(v);
+        while (full_[h]) {
+            if (keys_[h] == v) {
+                *fresh = false;
+                return h;
+            }
+            h = (h + 1) & mask_;
+        }
+        full_[h] = 1;
+        keys_[h] = v;
+        vals_[h] = 0;
+        used_++;
+        *fresh = true;
+        return h;
+    }
+    // Slot of a value known to be present.
+    size_t find(uint64_t v) const {
+        size_t h = home(v);
+        while (keys_[h] != v || !full_[h]) h = (h + 1) & mask_;
+        return h;
+    }
+    uint64_t &value(size_t slot) { return vals_[slot]; }
+
+  private:
+    void init(int lg) {
+        shift_ = 64 - lg;
+        mask_ = (size_t(1) << lg) - 1;
+        keys_.assign(size_t(1) << lg, 0);
+        vals_.assign(size_t(1) << lg, 0);
+        full_.assign(size_t(1) << lg, 0);
+        used_ = 0;
+    }
+    size_t home(uint64_t v) const { return size_t((v * 0x9E3779B97F4A7C15ull) >> shift_); }
+    void grow() {
+        std::vector<uint64_t> k, v;
+        std::vector<uint8_t> f;
+        k.swap(keys_), v.swap(vals_), f.swap(full_);
+        init(64 - shift_ + 1);
+        for (size_t i = 0; i < k.size(); i++) {
+            if (!f[i]) continue;
+            size_t h = home(k[i]);
+            while (full_[h]) h = (h + 1) & mask_;
+            full_[h] = 1, keys_[h] = k[i], vals_[h] = v[i];
+            used_++;
+        }
+    }
+    std::vector<uint64_t> keys_, vals_;
+    std::vector<uint8_t> full_;
+    size_t mask_ = 0, used_ = 0;
+    int shift_ = 64;
+};
+
+// Bump allocation for one call's hash-map nodes and bucket arrays; released with the arena.
+class NodeArena {
+  public:
+    void *take(size_t bytes, size_t align) {
+        size_t at = (used_ + align - 1) & ~(align - 1);
+        if (blocks_.empty() || at + bytes > cap_) {
+            cap_ = std::max<size_t>(size_t(1) << 20, bytes + align);
+            blocks_.emplace_back(new char[cap_]);
+            used_ = 0;
+            at = (reinterpret_cast<uintptr_t>(blocks_.back().get()) % align)
+                     ? align - reinterpret_cast<uintptr_t>(blocks_.back().get()) % align
+                     : 0;
+        }
+        used_ = at + bytes;
+        return blocks_.back().get() + at;
+    }
+
+  private:
+    std::vector<std::unique_ptr<char[]>> blocks_;
+    size_t used_ = 0, cap_ = 0;
+};
+
+template <typename T>
+struct ArenaAlloc {
+    using value_type = T;
+    NodeArena *arena;
+    explicit ArenaAlloc(NodeArena *a) : arena(a) {}
+    template <typename U>
+    ArenaAlloc(const ArenaAlloc<U> &o) : arena(o.arena) {}
+    T *allocate(size_t n) { return static_cast<T *>(arena->take(n * sizeof(T), alignof(T))); }
+    void deallocate(T *, size_t) {}
+    template <typename U>
+    bool operator==(const ArenaAlloc<U> &o) const { return arena == o.arena; }
+    template <typename U>
+    bool operator!=(const ArenaAlloc<U> &o) const { return arena != o.arena; }
+};
+
 template <typename Iterator>
 std::pair<std::vector<uint64_t>, std::vector<uint64_t>> ranks_and_dictionary(Iterator begin, uint64_t n) {
-    std::unordered_map<uint64_t, uint64_t> freq;
+    // Counts, and the distinct values in first-occurrence order.
+    FlatMap counts(std::min<uint64_t>(n, 1u << 16));
+    std::vector<uint64_t> first_seen;
     for (Iterator it = begin, end = begin + n; it != end; ++it) {
-        auto f = freq.find(*it);
-        if (f != freq.end()) f->second += 1;
-        else freq[*it] = 1;
+        bool fresh;
+        const size_t s = counts.find_or_insert(uint64_t(*it), &fresh);
+        if (fresh) first_seen.push_back(uint64_t(*it));
+        counts.value(s) += 1;
     }
+    // The reference's map, built by the same operator[] insertions in the same order.
+    NodeArena arena;
+    using Map = std::unordered_map<uint64_t, uint64_t, std::hash<uint64_t>, std::equal_to<uint64_t>,
+                                   ArenaAlloc<std::pair<const uint64_t, uint64_t>>>;
+    Map freq{ArenaAlloc<std::pair<const uint64_t, uint64_t>>(&arena)};
+    for (uint64_t v : first_seen) freq[v] = 1;
     std::vector<std::pair<uint64_t, uint64_t>> by_freq;
     by_freq.reserve(freq.size());
-    for (auto kv : freq) by_freq.emplace_back(kv.first, kv.second);
+    for (auto kv : freq) by_freq.emplace_back(kv.first, counts.value(counts.find(kv.first)));
     std::sort(by_freq.begin(), by_freq.end(), [](auto const &a, auto const &b) { return a.second > b.second; });
-    freq.clear();
     std::vector<uint64_t> dict;
-    dict.reserve(freq.size());
+    dict.reserve(by_freq.size());
     for (uint64_t i = 0; i != by_freq.size(); ++i) {
-        freq.insert({by_freq[i].first, i});
+        counts.value(counts.find(by_freq[i].first)) = i;  // the value's rank from here on
         dict.push_back(by_freq[i].first);
     }
     std::vector<uint64_t> ranks;
     ranks.reserve(n);
-    for (Iterator it = begin, end = begin + n; it != end; ++it) ranks.push_back(freq[*it]);
+    for (Iterator it = begin, end = begin + n; it != end; ++it) ranks.push_back(counts.value(counts.find(uint64_t(*it))));
     return {ranks, dict};
 }
 }  // namespace dict_detail

@@ -386,10 +386,15 @@ def encode(built: BuildResult, cfg: MPHFconfig, pilot_encoder: str = "interleave
     size, bpk = C.c_size_t(), C.c_double()
     args = (PILOT_ENCODERS[pilot_encoder], OFFSET_ENCODERS[offset_encoder], pil.ctypes.data, off.ctypes.data,
             built.partitions, C.byref(cfg.params), tradeoff)
-    check(_lib().phobic_encode(*args, None, 0, C.byref(size), C.byref(bpk)))
-    buf = np.zeros(size.value, np.uint8)
-    check(_lib().phobic_encode(*args, buf.ctypes.data, size.value, C.byref(size), C.byref(bpk)))
-    return buf.tobytes(), bpk.value
+    # One pass into a buffer sized for every encoder (at most 8 bytes per pilot and
+    # offset plus headers); a second pass only if the encoding is larger.
+    cap = 8 * (pil.size + off.size) + 64 * (built.buckets + 2) + (1 << 16)
+    buf = np.empty(cap, np.uint8)
+    check(_lib().phobic_encode(*args, buf.ctypes.data, cap, C.byref(size), C.byref(bpk)))
+    if size.value > cap:
+        buf = np.empty(size.value, np.uint8)
+        check(_lib().phobic_encode(*args, buf.ctypes.data, size.value, C.byref(size), C.byref(bpk)))
+    return buf[: size.value].tobytes(), bpk.value
 
 
 def encode_gpu(ctx: "Context", built: BuildResult, cfg: MPHFconfig, pilot_encoder: str = "interleaved_compact",
