@@ -135,8 +135,36 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
     const uint64_t hi = lo + a.chunk < a.total_keys ? lo + a.chunk : a.total_keys;
     SetCache sc;
     uint32_t bad_set = 0xFFFFFFFFu;
+    // u64 keys of one set (the plain build): all of an iteration's key loads are
+    // issued before any of them is hashed, so kUnroll loads per thread are in flight.
+    constexpr bool kRawU64 = KIND == PHOBIC_KEYS_U64 && !kReadMapped;
+    const bool raw_u64 = kRawU64 && a.nsets == 1;
+    const unsigned long long *keys64 = kRawU64 ? static_cast<const unsigned long long *>(a.sets[0].data) : nullptr;
+    const uint32_t parts0 = a.sets[0].partitions;
     for (uint64_t g0 = lo + threadIdx.x; g0 < hi; g0 += (uint64_t)kUnroll * kChunkThreads) {
         uint32_t gp[kUnroll], b[kUnroll], l1[kUnroll], l2[kUnroll];
+        if (raw_u64) {
+            uint64_t raw[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const uint64_t g = g0 + (uint64_t)u * kChunkThreads;
+                raw[u] = g < hi ? __ldg(keys64 + g) : 0ull;
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                const uint64_t g = g0 + (uint64_t)u * kChunkThreads;
+                gp[u] = 0xFFFFFFFFu;
+                if (g >= hi) continue;
+                const Key4 k = key_from_hash(xxh3::hash_u64(raw[u]));
+                gp[u] = partition_of(k.partitioner, parts0);
+                b[u] = bucket_of(k.bucketer, sf);
+                l1[u] = k.lower1, l2[u] = k.lower2;
+                if (!SCATTER) {
+                    if (b[u] >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = 0;
+                    if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+                }
+            }
+        } else {
 #pragma unroll
         for (int u = 0; u < kUnroll; u++) {
             const uint64_t g = g0 + (uint64_t)u * kChunkThreads;
@@ -150,6 +178,7 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
                     a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
                 }
             }
+        }
         }
         if constexpr (SCATTER) {
             uint32_t slot[kUnroll];
