@@ -46,7 +46,7 @@ struct SetCache {
 
 // Each thread takes kUnroll keys per iteration, kStride apart, so that their
 // loads and atomics are in flight together; the warp's loads stay coalesced.
-constexpr int kUnroll = 4;
+constexpr int kUnroll = 8;
 
 // Partition, bucket and lower pair of global key g.
 template <int KIND, bool READ_MAPPED>
