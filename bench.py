@@ -225,15 +225,38 @@ def run_ours(args) -> None:
     for _ in range(max(1, args.warmup)):
         ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
     grp.barrier()
+    # (a) one build at a time: each step's copy in, kernels and copy out in sequence
     e2e_wall, e2e_dev = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
         r2 = ctx.build(hks, cfg, out=(hp.data_ptr(), ho.data_ptr()))
         e2e_wall.append(time.perf_counter() - t0)
         e2e_dev.append(r2.timings["total"])
+    single_ms = grp.max(1e3 * sum(e2e_wall) / len(e2e_wall))
+    # (b) the same K steps on two contexts (two streams) from two host threads, as a
+    # caller with a stream of key sets runs them: one build's host copies overlap the
+    # other's kernels.  Every step still copies its keys in and its result out.
+    ctx_b = phobic.Context(local)
+    hp_b = torch.empty(parts * B, dtype=torch.int32).pin_memory()
+    ho_b = torch.empty(parts + 1, dtype=torch.int32).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        ctx_b.build(hks, cfg, out=(hp_b.data_ptr(), ho_b.data_ptr()))
+    lanes = [(ctx, hp, ho, (args.steps + 1) // 2), (ctx_b, hp_b, ho_b, args.steps // 2)]
+
+    def lane_run(c, p_, o_, k):
+        for _ in range(k):
+            c.build(hks, cfg, out=(p_.data_ptr(), o_.data_ptr()))
+
+    grp.barrier()
+    t0 = time.perf_counter()
+    th = [threading.Thread(target=lane_run, args=ln) for ln in lanes]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    e2e_ms = grp.max(1e3 * (time.perf_counter() - t0) / args.steps)
     clocks.__exit__(None, None, None)
-    e2e_ms = grp.max(1e3 * sum(e2e_wall) / len(e2e_wall))
-    same = bool((hp.numpy() == dp.cpu().numpy()).all())
+    same = bool((hp.numpy() == dp.cpu().numpy()).all()) and bool((hp_b.numpy() == dp.cpu().numpy()).all())
 
     # ---- host encoding of the result (Mphf::setData), C2's encoder: interleaved dictionary + diff compact
     built = phobic.BuildResult(hp.numpy().view(np.uint32), ho.numpy().view(np.uint32), parts, B)
@@ -254,6 +277,7 @@ def run_ours(args) -> None:
     encode_gpu_ms = min(gpu_enc)
 
     if rank != 0:
+        ctx_b.close()
         ctx.close()
         grp.close()
         return
@@ -295,7 +319,11 @@ def run_ours(args) -> None:
         "gpu_launches": int(stage["kernels"]) * args.steps,
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mkeys/s", "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 4 * (parts * B + parts + 1), "ms_per_step": e2e_ms,
-                "device_ms_per_step": statistics.mean(e2e_dev)},
+                "how": "phobic_build with pinned host keys and results, K steps on two contexts from two host "
+                       "threads (copies of one build overlap the other's kernels); wall clock",
+                "single": {"value": world * n / (single_ms / 1e3) / 1e6, "ms_per_step": single_ms,
+                           "device_ms_per_step": statistics.mean(e2e_dev),
+                           "how": "one build at a time on one context"}},
         "roofline": {"kernel": "k_search (K4)", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "bytes_per_key": K4_BYTES_PER_KEY,
@@ -312,6 +340,7 @@ def run_ours(args) -> None:
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
+    ctx_b.close()
     ctx.close()
     grp.close()
 
