@@ -31,8 +31,9 @@
 //
 // Buckets of at most 32 keys (nearly all of them) keep one key per lane in
 // registers and test collisions with __match_any_sync; for at most 8 keys the
-// offset search also keeps every slot in registers, for 9..32 keys it reads them
-// from shared memory four at a time.  Larger buckets read their keys from the
+// offset search also keeps every slot in registers (as 4 or 8 slots, the unused
+// ones repeating slot 0), for 9..32 keys it reads them from shared memory four at
+// a time.  Larger buckets read their keys from the
 // bucket-ordered copy in global memory and stage their slots in shared memory.
 #include "kernels.cuh"
 
@@ -292,9 +293,9 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
         const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
         uint32_t o;
         if (s <= 8 && rounds <= 4) {
-            if (s == 1) o = first_free_offset_unr<1>(ws.occ, hp, ps, rounds, lane);
-            else if (s == 2) o = first_free_offset_unr<2>(ws.occ, hp, ps, rounds, lane);
-            else if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane);
+            // Two unrolled variants only: a smaller hot loop (fewer instruction-cache
+            // misses) outweighs the repeated slot of buckets of one or two keys.
+            if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane);
             else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane);
         } else if (s == 1) o = first_free_offset_reg<1>(ws.occ, hp, ps, lane);
         else if (s == 2) o = first_free_offset_reg<2>(ws.occ, hp, ps, lane);
