@@ -249,7 +249,7 @@ __device__ __forceinline__ bool scan_round(const uint32_t (&hb)[K], const uint32
     return true;
 }
 
-// first_free_offset_reg for ps <= 4096: the (at most four) rounds unrolled, each
+// first_free_offset_reg for ps <= 3072: the (at most three) rounds unrolled, each
 // key's window address formed once per call with the lane's word offset included,
 // so a round reads at a constant 128 R bytes further.  Dead lanes (offsets >= ps)
 // read inside the padded bitmap (bitmap_words) and are masked.
@@ -267,7 +267,6 @@ __device__ __forceinline__ uint32_t first_free_offset_unr(const uint32_t *occ, u
     if (scan_round<K, 0>(hb, v, ps, lane, &o)) return o;
     if (rounds > 1 && scan_round<K, 1>(hb, v, ps, lane, &o)) return o;
     if (rounds > 2 && scan_round<K, 2>(hb, v, ps, lane, &o)) return o;
-    if (rounds > 3 && scan_round<K, 3>(hb, v, ps, lane, &o)) return o;
     return kNone;
 }
 
@@ -292,14 +291,12 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
         }
         const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
         uint32_t o;
-        if (s <= 8 && rounds <= 4) {
+        if (s <= 8 && rounds <= 3) {
             // Two unrolled variants only: a smaller hot loop (fewer instruction-cache
             // misses) outweighs the repeated slot of buckets of one or two keys.
             if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane);
             else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane);
-        } else if (s == 1) o = first_free_offset_reg<1>(ws.occ, hp, ps, lane);
-        else if (s == 2) o = first_free_offset_reg<2>(ws.occ, hp, ps, lane);
-        else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane);
+        } else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane);
         else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane);
         else {
             if (lane < (int)padded) ws.hs[lane] = hp;
