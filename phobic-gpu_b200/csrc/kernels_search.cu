@@ -270,20 +270,25 @@ __device__ __forceinline__ uint32_t first_free_offset_unr(const uint32_t *occ, u
     return kNone;
 }
 
+// Whether two keys of a bucket of s <= 32 keys (key `lane` in L) are identical.
+// Reached only when a bucket's pilot counter gets to kDupCheckAt, so it is kept
+// out of line, away from the instructions of the search loop.
+__device__ __noinline__ bool has_duplicate_key(uint2 L, uint32_t s, int lane) {
+    bool d = false;
+    for (uint32_t t = 0; t + 1 < s; t++) {
+        uint32_t x = __shfl_sync(kFullMask, L.x, t), y = __shfl_sync(kFullMask, L.y, t);
+        d |= lane < (int)s && lane > (int)t && L.x == x && L.y == y;
+    }
+    return __any_sync(kFullMask, d);
+}
+
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
 __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
                                                 uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
     const bool mine = lane < (int)s;
     const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
-        if (k == kDupCheckAt && s > 1) {
-            bool d = false;
-            for (uint32_t t = 0; t + 1 < s; t++) {
-                uint32_t x = __shfl_sync(kFullMask, L.x, t), y = __shfl_sync(kFullMask, L.y, t);
-                d |= mine && lane > (int)t && L.x == x && L.y == y;
-            }
-            if (__any_sync(kFullMask, d)) return PHOBIC_ERR_DUPLICATE_KEY;
-        }
+        if (k == kDupCheckAt && s > 1 && has_duplicate_key(L, s, lane)) return PHOBIC_ERR_DUPLICATE_KEY;
         const uint32_t h = mine ? fm.mod(pilot_hash(L.x, L.y, k)) : (0x80000000u | lane);
         if (s > 1) {
             uint32_t m = __match_any_sync(kFullMask, h);
