@@ -81,7 +81,53 @@ int query_impl(const uint32_t *pilots, const uint32_t *offsets, uint32_t partiti
     return 0;
 }
 
+// Encode with setData, serialise, load the bytes into a fresh MPHF with
+// loadEncoded and query every key through both: 0 when every slot agrees and the
+// reloaded function re-serialises to the same bytes, 1 on a difference, 2 when
+// loadEncoded rejects the bytes, 3 when it accepts them with one byte missing.
+template <typename PilotEnc, typename OffEnc>
+int roundtrip_impl(const uint32_t *pilots, const uint32_t *offsets, uint32_t partitions, double lambda, uint32_t P,
+                   const uint64_t *keys, uint64_t n) {
+    MPHFconfig config(lambda, P);
+    std::vector<uint32_t> pil(pilots, pilots + (size_t)partitions * config.bucketCountPerPartition);
+    std::vector<uint32_t> offs(offsets, offsets + partitions + 1);
+    MPHF<PilotEnc, OffEnc, xxhash> f, g, h;
+    f.setData(pil, offs, partitions, config);
+    ByteSaver s;
+    f.getPilotEncoder().visit(s);
+    f.getPartitionOffsetEncoder().visit(s);
+    if (!g.loadEncoded(s.out.data(), s.out.size(), partitions, config)) return 2;
+    if (!s.out.empty() && h.loadEncoded(s.out.data(), s.out.size() - 1, partitions, config)) return 3;
+    for (uint64_t i = 0; i < n; i++)
+        if (f(keys[i]) != g(keys[i])) return 1;
+    ByteSaver t;
+    g.getPilotEncoder().visit(t);
+    g.getPartitionOffsetEncoder().visit(t);
+    return t.out == s.out ? 0 : 1;
+}
+
 }  // namespace
+
+extern "C" int mine_roundtrip(int pilot_kind, int offset_kind, const uint32_t *pilots, const uint32_t *offsets,
+                              uint32_t partitions, double lambda, uint32_t P, const uint64_t *keys, uint64_t n) {
+    const bool direct = offset_kind == 1;
+    if (pilot_kind == 0)
+        return direct ? roundtrip_impl<interleaved_encoder<compact>, direct_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n)
+                      : roundtrip_impl<interleaved_encoder<compact>, diff_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n);
+    if (pilot_kind == 3)
+        return direct ? roundtrip_impl<mono_encoder<compact>, direct_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n)
+                      : roundtrip_impl<mono_encoder<compact>, diff_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n);
+    if (pilot_kind == 1)
+        return direct ? roundtrip_impl<interleaved_encoder<dictionary>, direct_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n)
+                      : roundtrip_impl<interleaved_encoder<dictionary>, diff_partition_encoder<compact>>(
+                            pilots, offsets, partitions, lambda, P, keys, n);
+    return -1;
+}
 
 extern "C" size_t mine_encode(int pilot_kind, int offset_kind, const uint32_t *pilots, const uint32_t *offsets,
                               uint32_t partitions, double lambda, uint32_t P, float tradeoff, uint8_t *out, size_t cap,

@@ -31,6 +31,8 @@ def mine(tmp_path_factory):
                                 C.c_float, C.c_void_p, C.c_size_t, C.POINTER(C.c_double)]
     lib.mine_query.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32, C.c_void_p,
                                C.c_uint64, C.c_void_p]
+    lib.mine_roundtrip.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
+                                   C.c_void_p, C.c_uint64]
     return lib
 
 
@@ -113,3 +115,20 @@ def test_abi_encode_matches_reference_golden(phobic, golden):
         for off_name in ("diff", "direct"):
             data, bpk = phobic.encode(built, cfg, name, off_name)
             assert hashlib.sha256(data).hexdigest() == want[f"{name}+{off_name}"]["sha256"], (name, off_name)
+
+
+@pytest.mark.parametrize("kind", [0, 1, 3])
+@pytest.mark.parametrize("off_kind", [0, 1])
+@pytest.mark.parametrize("n", [1, 2049, 60_000])
+def test_load_encoded_bytes_round_trip(mine, kind, off_kind, n):
+    """MPHF::loadEncoded (the state setData leaves, read back from the encoders' bytes,
+    as MPHFbuilder does with the bytes of phobic_encode_gpu) answers every key like
+    the function it was saved from, re-serialises to the same bytes, and rejects a
+    truncated byte string."""
+    lam, P = 6.0, 2048
+    keys = O.splitmix64(40 + n, n)
+    B, f = O.config(lam, P)
+    r = O.build(O.hash_keys(keys, "u64"), P, B, f)
+    rc = mine.mine_roundtrip(kind, off_kind, r["pilots"].ctypes.data, r["offsets"].ctypes.data, r["partitions"],
+                             lam, P, keys.ctypes.data, n)
+    assert rc == 0, rc
