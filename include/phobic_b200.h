@@ -124,6 +124,11 @@ PHOBIC_API phobic_status phobic_ctx_destroy(phobic_ctx *ctx);
 PHOBIC_API const char *phobic_last_error(const phobic_ctx *ctx);
 /* Device bytes the context's pools hold now. */
 PHOBIC_API uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx);
+/* Caps the device memory of the context's build pool (0 = no cap).  A build whose
+ * pool would exceed the cap fails with PHOBIC_ERR_OOM before any allocation is
+ * attempted, and the context stays usable; a pool already above the cap is freed.
+ * The reference allocates per build without a limit (memory.cpp:40-90). */
+PHOBIC_API phobic_status phobic_ctx_set_memory_limit(phobic_ctx *ctx, uint64_t bytes);
 /* The context's CUDA stream (a cudaStream_t): every kernel of its builds runs on it, so
  * callers can order their own work and time builds with events on this stream. */
 PHOBIC_API void *phobic_ctx_stream(const phobic_ctx *ctx);

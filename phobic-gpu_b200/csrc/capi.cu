@@ -102,6 +102,16 @@ const char *phobic_last_error(const phobic_ctx *ctx) { return ctx ? ctx->last_er
 
 uint64_t phobic_ctx_device_bytes(const phobic_ctx *ctx) { return ctx ? ctx->w.arena.capacity() : 0; }
 
+phobic_status phobic_ctx_set_memory_limit(phobic_ctx *ctx, uint64_t bytes) {
+    if (!ctx) return PHOBIC_ERR_INVALID;
+    if (cudaSetDevice(ctx->w.device) != cudaSuccess) {
+        cudaGetLastError();
+        return PHOBIC_ERR_CUDA;
+    }
+    ctx->w.arena.set_limit(bytes);
+    return PHOBIC_OK;
+}
+
 void *phobic_ctx_stream(const phobic_ctx *ctx) { return ctx ? static_cast<void *>(ctx->w.stream) : nullptr; }
 
 uint64_t phobic_build_bytes_needed(const phobic_keys *keys, const phobic_params *params) {

@@ -22,15 +22,26 @@
 #include <thread>
 
 #include "kernels.cuh"
+#include "nvtx3/nvToolsExt.h"
 
 namespace phobicb200 {
+
+namespace {
+// NVTX range for the host side of one stage (launches and copies), named with the
+// reference's stage labels; profilers show it beside the kernels it launched.
+struct StageRange {
+    explicit StageRange(const char *name) { nvtxRangePushA(name); }
+    ~StageRange() { nvtxRangePop(); }
+};
+}  // namespace
 
 // ------------------------------------------------------------------ memory
 
 cudaError_t DeviceArena::reserve(size_t bytes) {
     if (bytes <= cap_) return cudaSuccess;
-    release();
     size_t want = align256(bytes);
+    if (limit_ && want > limit_) return cudaErrorMemoryAllocation;
+    release();
     cudaError_t e = cudaMalloc(&base_, want);
     if (e != cudaSuccess) {
         base_ = nullptr;
@@ -358,20 +369,32 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
                (uint32_t)M, plan.stride, plan.chunk};
     // K1, scan, size check, two partition passes, search; none when there are no keys.
     w.pending_kernels = N ? 6 : 0;
-    PHB_TRY(launch_map_count(kind, ma, plan, s), "K1 map_count");
+    {
+        StageRange r("bucket_sizes (K1)");
+        PHB_TRY(launch_map_count(kind, ma, plan, s), "K1 map_count");
+    }
     PHB_TRY(cudaEventRecord(w.ev[2], s), "event");
     ScanArgs sa{d_count, d_G, nullptr, (uint32_t)MS, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles), nsets,
                 d_err, 0};
-    PHB_TRY(launch_scan(sa, s), "K2 scan");
+    {
+        StageRange r("partition_offsets (K2)");
+        PHB_TRY(launch_scan(sa, s), "K2 scan");
+    }
     const uint32_t wshift = part_wshift(M);
     PartArgs pa{d_inter, d_bincur, d_pcur, wshift, (uint32_t)((M + (1ull << wshift) - 1) >> wshift)};
     PHB_TRY(launch_check_sizes(d_G, (uint32_t)M, plan.stride, cap, d_pb, nsets, d_err, &pa, s), "K2 size check");
     PHB_TRY(cudaEventRecord(w.ev[3], s), "event");
-    PHB_TRY(launch_partition(kind, ma, pa, w.sm_count, s), "K3 partition");
+    {
+        StageRange r("key_redistribution (K3)");
+        PHB_TRY(launch_partition(kind, ma, pa, w.sm_count, s), "K3 partition");
+    }
     PHB_TRY(cudaEventRecord(w.ev[4], s), "event");
     SearchArgs qa{d_desc, d_pb, nsets, (uint32_t)M, d_G, plan.stride, d_lowers, d_bkt, d_sorted, d_dbg_sizes, B, cap,
                   k_max, d_queue, d_err};
-    PHB_TRY(launch_search(qa, w.sm_count, s), "K4 search");
+    {
+        StageRange r("search (K4)");
+        PHB_TRY(launch_search(qa, w.sm_count, s), "K4 search");
+    }
     PHB_TRY(cudaEventRecord(w.ev[5], s), "event");
 
     PHB_TRY(cudaMemcpyAsync(w.pending_err, d_err, 8 * nsets, cudaMemcpyDeviceToHost, s), "D2H status");
@@ -415,7 +438,11 @@ static const char *error_text(uint32_t code) {
 }
 
 phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t, std::string *err) {
-    phobic_status st = wait_event(w.ev[6], w.timeout_ms, err);
+    phobic_status st;
+    {
+        StageRange r("wait for the build");
+        st = wait_event(w.ev[6], w.timeout_ms, err);
+    }
     if (st != PHOBIC_OK) return st;
     if (t) {
         t->input_transfer = elapsed(w.ev[0], w.ev[1]);

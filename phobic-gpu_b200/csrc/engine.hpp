@@ -18,15 +18,22 @@ namespace phobicb200 {
 class DeviceArena {
   public:
     ~DeviceArena() { release(); }
+    // Grows the pool to at least `bytes`; cudaErrorMemoryAllocation, without calling
+    // cudaMalloc, when that exceeds the limit (if one is set).
     cudaError_t reserve(size_t bytes);
     void reset() { used_ = 0; }
     void *take(size_t bytes);
     size_t capacity() const { return cap_; }
     void release();
+    // Upper bound on the pool's size; 0 = none.  A pool above a new limit is released.
+    void set_limit(size_t bytes) {
+        limit_ = bytes;
+        if (limit_ && cap_ > limit_) release();
+    }
 
   private:
     char *base_ = nullptr;
-    size_t cap_ = 0, used_ = 0;
+    size_t cap_ = 0, used_ = 0, limit_ = 0;
 };
 
 // A grow-only pinned host buffer.

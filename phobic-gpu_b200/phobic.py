@@ -125,6 +125,7 @@ def _lib() -> C.CDLL:
         "phobic_last_error": (C.c_char_p, [P]),
         "phobic_ctx_device_bytes": (U64, [P]),
         "phobic_ctx_stream": (P, [P]),
+        "phobic_ctx_set_memory_limit": (I32, [P, U64]),
         "phobic_build_bytes_needed": (U64, [C.POINTER(Keys), C.POINTER(Params)]),
         "phobic_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(Timings)]),
         "phobic_build_u64": (I32, [P, P, U64, C.POINTER(Params), P, P, C.POINTER(Timings)]),
@@ -338,6 +339,10 @@ class Context:
         check(_lib().phobic_query(self.handle, C.byref(k), C.byref(cfg.params), built.partitions, C.byref(res),
                                   pos.ctypes.data), self)
         return pos[: ks.n]
+
+    def set_memory_limit(self, nbytes: int) -> None:
+        """Cap the device memory of this context's build pool (0 = no cap)."""
+        check(_lib().phobic_ctx_set_memory_limit(self.handle, nbytes), self)
 
     def stalled_wait(self, wait_ms: int) -> int:
         """Status recorded by a kernel whose bounded wait on a never-set flag ran out."""

@@ -35,3 +35,20 @@ def test_errors_leave_other_sets_of_a_batch_intact(phobic):
         assert st == [0, phobic.ERR_DUPLICATE_KEY, 0, 0]
         for keys, res in zip(good, [outs[0], outs[2], outs[3]]):
             assert ctx.verify(keys, cfg, res) == 0
+
+
+def test_memory_limit_gives_oom_and_context_survives(phobic):
+    """An allocation failure injected on the host: the context's memory cap makes the
+    build fail with PHOBIC_ERR_OOM before cudaMalloc is called; lifting the cap, the
+    same context builds the same keys correctly."""
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(61, 200_000)
+    with phobic.Context(0) as c:
+        c.set_memory_limit(1 << 20)
+        with pytest.raises(phobic.PhobicError) as e:
+            c.build(keys, cfg)
+        assert e.value.status == phobic.ERR_OOM
+        assert c.device_bytes() <= 1 << 20
+        c.set_memory_limit(0)
+        got = c.build(keys, cfg)
+        assert c.verify(keys, cfg, got) == 0
