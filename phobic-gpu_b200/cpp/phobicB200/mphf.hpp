@@ -12,6 +12,31 @@
 
 namespace phobicgpu {
 
+// Writes serialised fields in visit order: a trivially copyable value as its bytes,
+// a vector as its size_t count followed by its elements.
+struct ByteSaver {
+    std::vector<uint8_t> out;
+    void put(const void *p, size_t n) {
+        const uint8_t *b = static_cast<const uint8_t *>(p);
+        out.insert(out.end(), b, b + n);
+    }
+    template <typename T>
+    void visit(std::vector<T> &v) {
+        size_t n = v.size();
+        put(&n, sizeof(n));
+        if constexpr (std::is_trivially_copyable_v<T>) {
+            if (n) put(v.data(), n * sizeof(T));
+        } else {
+            for (auto &e : v) visit(e);
+        }
+    }
+    template <typename T>
+    void visit(T &v) {
+        if constexpr (std::is_trivially_copyable_v<T>) put(&v, sizeof(T));
+        else v.visit(*this);
+    }
+};
+
 // Reads serialised fields in visit order: a trivially copyable value as its bytes,
 // a vector as its size_t count followed by its elements.
 struct ByteLoader {
@@ -99,6 +124,31 @@ class MPHF {
         pilots.set_shape(parts, config.bucketCountPerPartition);
         partitionOffsets.set_shape(config.partitionSize);
         ByteLoader loader{bytes, size};
+        pilots.visit(loader);
+        partitionOffsets.visit(loader);
+        return loader.ok && loader.pos == size;
+    }
+
+    // The whole function as bytes, in visit order: partition count, fulcrum table,
+    // pilot encoder, partition-offset encoder (vectors as a size_t count followed
+    // by their elements).
+    std::vector<uint8_t> save() {
+        ByteSaver saver;
+        visit(saver);
+        return std::move(saver.out);
+    }
+
+    // The function saved by save().  The bytes hold everything but the partition
+    // size, which the offset encoder's expected-offset line needs; the bucket count
+    // per partition is the last fulcrum >> 16 (mphf_config.h:44-55).  False when the
+    // bytes are not one saved function.
+    bool load(const uint8_t *bytes, size_t size, uint32_t partition_size) {
+        ByteLoader loader{bytes, size};
+        loader.visit(partitions);
+        loader.visit(fulcs);
+        if (!loader.ok || fulcs.size() != phobicb200::kFulcrums) return false;
+        pilots.set_shape(partitions, fulcs.back() >> 16);
+        partitionOffsets.set_shape(partition_size);
         pilots.visit(loader);
         partitionOffsets.visit(loader);
         return loader.ok && loader.pos == size;

@@ -16,6 +16,7 @@
 #include "phobicB200/builder.hpp"
 #include "phobicB200/config.hpp"
 #include "phobicB200/encoders.hpp"
+#include "phobicB200/layout.hpp"
 #include "phobicB200/mphf.hpp"
 
 namespace phobicgpu {

@@ -11,29 +11,6 @@ using namespace phobicgpu;
 
 namespace {
 
-struct ByteSaver {
-    std::vector<uint8_t> out;
-    void put(const void *p, size_t n) {
-        const uint8_t *b = static_cast<const uint8_t *>(p);
-        out.insert(out.end(), b, b + n);
-    }
-    template <typename T>
-    void visit(std::vector<T> &v) {
-        size_t n = v.size();
-        put(&n, sizeof(n));
-        if constexpr (std::is_trivially_copyable_v<T>) {
-            if (n) put(v.data(), n * sizeof(T));
-        } else {
-            for (auto &e : v) visit(e);
-        }
-    }
-    template <typename T>
-    void visit(T &v) {
-        if constexpr (std::is_trivially_copyable_v<T>) put(&v, sizeof(T));
-        else v.visit(*this);
-    }
-};
-
 // An MPHFconfig with the caller's table (the encoders read partitionSize and B).
 MPHFconfig config_from(const phobic_params *p) {
     MPHFconfig c(double(p->partition_size) / double(p->buckets), p->partition_size);

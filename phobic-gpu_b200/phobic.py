@@ -422,6 +422,49 @@ def encode_gpu(ctx: "Context", built: BuildResult, cfg: MPHFconfig, pilot_encode
     return buf[: size.value].tobytes(), bpk.value, size.value
 
 
+# ------------------------------------------------------------------ pilot-layout files
+
+_LAYOUT_MAGIC = b"PHBLAYT1"
+
+
+def save_layout(path, built: BuildResult, cfg: MPHFconfig) -> None:
+    """Write a build's pilots and partition offsets (before any encoding) in the file
+    layout of the C++ layer's savePilotLayout: magic, n, partitions, buckets, P, then
+    the bucket-major pilots and the offsets, all little-endian."""
+    pil = np.ascontiguousarray(_host(built.pilots), np.uint32).reshape(-1)
+    off = np.ascontiguousarray(_host(built.partition_offsets), np.uint32).reshape(-1)
+    if pil.size != built.buckets * built.partitions or off.size != built.partitions + 1:
+        raise ValueError("result arrays do not match their partition and bucket counts")
+    head = np.array([built.partitions, built.buckets, cfg.partitionSize, 0], "<u4")
+    with open(path, "wb") as f:
+        f.write(_LAYOUT_MAGIC)
+        f.write(np.array([int(off[-1])], "<u8").tobytes())
+        f.write(head.tobytes())
+        f.write(pil.astype("<u4", copy=False).tobytes())
+        f.write(off.astype("<u4", copy=False).tobytes())
+
+
+def load_layout(path) -> tuple[BuildResult, int]:
+    """Read a file written by save_layout (or savePilotLayout): (result, partition size)."""
+    data = open(path, "rb").read()
+    if data[:8] != _LAYOUT_MAGIC or len(data) < 32:
+        raise ValueError("not a pilot-layout file")
+    n = int(np.frombuffer(data, "<u8", 1, 8)[0])
+    parts, buckets, psize, _ = (int(x) for x in np.frombuffer(data, "<u4", 4, 16))
+    npil = parts * buckets
+    if len(data) != 32 + 4 * (npil + parts + 1):
+        raise ValueError("pilot-layout file size does not match its header")
+    pil = np.frombuffer(data, "<u4", npil, 32).astype(np.uint32)
+    off = np.frombuffer(data, "<u4", parts + 1, 32 + 4 * npil).astype(np.uint32)
+    if off[0] != 0 or int(off[-1]) != n:
+        raise ValueError("pilot-layout file has inconsistent partition offsets")
+    return BuildResult(pil, off, parts, buckets), psize
+
+
+def _host(x):
+    return x.cpu().numpy().view(np.uint32) if hasattr(x, "cpu") else x
+
+
 # ------------------------------------------------------------------ batch and serving
 
 def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None = None, outs_in: list | None = None):

@@ -11,29 +11,6 @@ using namespace phobicgpu;
 
 namespace {
 
-struct ByteSaver {
-    std::vector<uint8_t> out;
-    void put(const void *p, size_t n) {
-        const uint8_t *b = static_cast<const uint8_t *>(p);
-        out.insert(out.end(), b, b + n);
-    }
-    template <typename T>
-    void visit(std::vector<T> &v) {
-        size_t n = v.size();
-        put(&n, sizeof(n));
-        if constexpr (std::is_trivially_copyable_v<T>) {
-            if (n) put(v.data(), n * sizeof(T));
-        } else {
-            for (auto &e : v) visit(e);
-        }
-    }
-    template <typename T>
-    void visit(T &v) {
-        if constexpr (std::is_trivially_copyable_v<T>) put(&v, sizeof(T));
-        else v.visit(*this);
-    }
-};
-
 template <typename PilotEnc, typename OffEnc>
 size_t encode_impl(const uint32_t *pilots, const uint32_t *offsets, uint32_t partitions, double lambda, uint32_t P,
                    uint8_t *out, size_t cap, double *bpk, float tradeoff) {
@@ -127,6 +104,25 @@ extern "C" int mine_roundtrip(int pilot_kind, int offset_kind, const uint32_t *p
                       : roundtrip_impl<interleaved_encoder<dictionary>, diff_partition_encoder<compact>>(
                             pilots, offsets, partitions, lambda, P, keys, n);
     return -1;
+}
+
+// A pilot-layout file (written by the Python binding) loaded with loadPilotLayout,
+// encoded with setData (interleaved compact + diff compact), saved with
+// MPHF::save, loaded again with MPHF::load, and every key queried through both:
+// 0 when all agree, 1 on a difference, 2 when the layout file is rejected, 3 when
+// MPHF::load rejects the saved bytes, 4 when it accepts them truncated.
+extern "C" int mine_layout_and_save(const char *path, double lambda, const uint64_t *keys, uint64_t n) {
+    PilotLayout l;
+    if (!loadPilotLayout(path, &l)) return 2;
+    MPHFconfig config(lambda, l.partition_size);
+    FastQueryMphf f, g, h;
+    f.setData(l.pilots, l.offsets, l.partitions, config);
+    std::vector<uint8_t> bytes = f.save();
+    if (!g.load(bytes.data(), bytes.size(), l.partition_size)) return 3;
+    if (!bytes.empty() && h.load(bytes.data(), bytes.size() - 1, l.partition_size)) return 4;
+    for (uint64_t i = 0; i < n; i++)
+        if (f(keys[i]) != g(keys[i])) return 1;
+    return g.save() == bytes ? 0 : 1;
 }
 
 extern "C" size_t mine_encode(int pilot_kind, int offset_kind, const uint32_t *pilots, const uint32_t *offsets,

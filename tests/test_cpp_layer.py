@@ -33,6 +33,7 @@ def mine(tmp_path_factory):
                                C.c_uint64, C.c_void_p]
     lib.mine_roundtrip.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_uint32, C.c_double, C.c_uint32,
                                    C.c_void_p, C.c_uint64]
+    lib.mine_layout_and_save.argtypes = [C.c_char_p, C.c_double, C.c_void_p, C.c_uint64]
     return lib
 
 
@@ -132,3 +133,27 @@ def test_load_encoded_bytes_round_trip(mine, kind, off_kind, n):
     rc = mine.mine_roundtrip(kind, off_kind, r["pilots"].ctypes.data, r["offsets"].ctypes.data, r["partitions"],
                              lam, P, keys.ctypes.data, n)
     assert rc == 0, rc
+
+
+@pytest.mark.parametrize("n,lam,P", [(1, 5.0, 2048), (70_000, 7.0, 2500)])
+def test_pilot_layout_file_and_mphf_save_load(mine, phobic, tmp_path, n, lam, P):
+    """A build's pilot layout written by the Python binding is read by the C++
+    layer's loadPilotLayout, encoded, saved with MPHF::save and loaded with
+    MPHF::load: every key maps to the same slot, the reloaded function saves the
+    same bytes, truncated bytes are rejected; the Python reader returns the arrays."""
+    keys = O.splitmix64(77 + n, n)
+    B, f = O.config(lam, P)
+    r = O.build(O.hash_keys(keys, "u64"), P, B, f)
+    cfg = phobic.MPHFconfig(lam, P)
+    built = phobic.BuildResult(r["pilots"], r["offsets"], r["partitions"], B)
+    path = tmp_path / "layout.bin"
+    phobic.save_layout(path, built, cfg)
+    back, psize = phobic.load_layout(path)
+    assert psize == P and back.partitions == r["partitions"] and back.buckets == B
+    assert (back.pilots == r["pilots"]).all() and (back.partition_offsets == r["offsets"]).all()
+    assert mine.mine_layout_and_save(str(path).encode(), lam, keys.ctypes.data, n) == 0
+    data = path.read_bytes()
+    path.write_bytes(data[:-4])
+    with pytest.raises(ValueError):
+        phobic.load_layout(path)
+    assert mine.mine_layout_and_save(str(path).encode(), lam, keys.ctypes.data, n) == 2
