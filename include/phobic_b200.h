@@ -161,6 +161,14 @@ PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *
  * scheduled, so the next tile's look-back waits on a flag that nothing sets.  The
  * kernel's bounded wait (wait_ms) must give up and record PHOBIC_ERR_TIMEOUT, which is
  * returned in *observed; the context stays usable afterwards. */
+/* The bounds checks of the checked library (libphobic_b200_checked.so, built with
+ * -DPHOBIC_CHECKED): *compiled = 1 there, 0 in the normal library.  lines[0..2] = the
+ * source line of the first failed check in the key-mapping, partition and search
+ * kernels (0 = none failed).  A failed check skips its memory access instead of
+ * trapping.  reset != 0 clears the records.  Stands in for a memory checker, which is
+ * not available on every machine (it has no counterpart in the reference, which
+ * relies on Vulkan validation layers, src/app/app.cpp:96-108). */
+PHOBIC_API phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *lines, int reset);
 PHOBIC_API phobic_status phobic_debug_stalled_wait(phobic_ctx *ctx, uint32_t wait_ms, phobic_status *observed);
 
 /* ------------------------------------------------------------------ encoding

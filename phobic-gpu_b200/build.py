@@ -18,6 +18,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build"
 LIB = PKG / "lib" / "libphobic_b200.so"
+# The bounds-checked variant (-DPHOBIC_CHECKED): kernels check their indexes and
+# record the first failing check instead of making the access.
+OBJ_CHECKED = PKG / "_build_checked"
+LIB_CHECKED = PKG / "lib" / "libphobic_b200_checked.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -43,8 +47,8 @@ def _stale(obj: Path, src: Path, newest_header: float) -> bool:
     return not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header)
 
 
-def _compile(src: Path, extra: list[str]) -> Path:
-    obj = OBJ / (src.stem + ".o")
+def _compile(src: Path, extra: list[str], objdir: Path = OBJ) -> Path:
+    obj = objdir / (src.stem + ".o")
     cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", str(src), "-o", str(obj)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
@@ -54,27 +58,29 @@ def _compile(src: Path, extra: list[str]) -> Path:
     return obj
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False) -> Path:
-    OBJ.mkdir(exist_ok=True)
-    LIB.parent.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False, checked: bool = False) -> Path:
+    objdir, lib = (OBJ_CHECKED, LIB_CHECKED) if checked else (OBJ, LIB)
+    objdir.mkdir(exist_ok=True)
+    lib.parent.mkdir(exist_ok=True)
     sources = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
     newest = max((h.stat().st_mtime for h in _headers()), default=0.0)
-    todo = [s for s in sources if force or _stale(OBJ / (s.stem + ".o"), s, newest)]
-    extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+    todo = [s for s in sources if force or _stale(objdir / (s.stem + ".o"), s, newest)]
+    extra = (["-Xptxas", "-v"] if ptxas_verbose else []) + (["-DPHOBIC_CHECKED"] if checked else [])
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        for obj in ex.map(lambda s: _compile(s, extra), todo):
+        for obj in ex.map(lambda s: _compile(s, extra, objdir), todo):
             if verbose:
                 print("compiled", obj.name)
-    objs = [OBJ / (s.stem + ".o") for s in sources]
-    if todo or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lpthread", "-lgomp"]
+    objs = [objdir / (s.stem + ".o") for s in sources]
+    if todo or not lib.exists() or lib.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lpthread", "-lgomp"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stderr}")
         if verbose:
-            print("linked", LIB)
-    return LIB
+            print("linked", lib)
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose=True, force="--force" in sys.argv, ptxas_verbose="--ptxas" in sys.argv)
+    build(verbose=True, force="--force" in sys.argv, ptxas_verbose="--ptxas" in sys.argv,
+          checked="--checked" in sys.argv)

@@ -260,6 +260,23 @@ phobic_status phobic_ctx_result(phobic_ctx *ctx, uint32_t buckets, uint32_t part
     return PHOBIC_OK;
 }
 
+phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *lines, int reset) {
+    if (!ctx || !compiled || !lines) return PHOBIC_ERR_INVALID;
+    if (cudaSetDevice(ctx->w.device) != cudaSuccess || cudaStreamSynchronize(ctx->w.stream) != cudaSuccess) {
+        cudaGetLastError();
+        return PHOBIC_ERR_CUDA;
+    }
+#ifdef PHOBIC_CHECKED
+    *compiled = 1;
+#else
+    *compiled = 0;
+#endif
+    lines[0] = check_line_map(reset != 0);
+    lines[1] = check_line_part(reset != 0);
+    lines[2] = check_line_search(reset != 0);
+    return PHOBIC_OK;
+}
+
 phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
                             const phobic_result *built, uint64_t *bad) {
     if (!ctx || !keys || !params || !bad) return PHOBIC_ERR_INVALID;

@@ -51,6 +51,33 @@ struct FastMod {
     }
 };
 
+// Bounds checks of the checked build (-DPHOBIC_CHECKED).  PHB_CHECK(cond) guards one
+// shared- or global-memory access: in the checked build a false condition records
+// the check's source line in this translation unit's status word (the first failure
+// is kept) and the access is skipped; in the normal build it is `true` and compiles
+// away.  Nothing traps: the kernel runs on and the host reads the word afterwards.
+#ifdef PHOBIC_CHECKED
+static __device__ unsigned int g_check_line;
+__device__ __forceinline__ bool phb_check(bool ok, unsigned int line) {
+    if (!ok) atomicCAS(&g_check_line, 0u, line);
+    return ok;
+}
+#define PHB_CHECK(cond) ::phobicb200::phb_check((cond), __LINE__)
+// This translation unit's status word (0 = no failed check); reset clears it.
+static inline unsigned int read_check_line(bool reset) {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_check_line, sizeof(v)) != cudaSuccess) return 0xFFFFFFFFu;
+    if (reset) {
+        const unsigned int z = 0;
+        cudaMemcpyToSymbol(g_check_line, &z, sizeof(z));
+    }
+    return v;
+}
+#else
+#define PHB_CHECK(cond) true
+static inline unsigned int read_check_line(bool) { return 0; }
+#endif
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -186,6 +186,11 @@ cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int 
 // PHOBIC_ERR_TIMEOUT (failure-detection tests).
 cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t st);
 cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st);
+// First failed bounds check of each kernel file in the checked build (source line, 0 =
+// none; always 0 in the normal build); reset clears it.
+unsigned int check_line_map(bool reset);
+unsigned int check_line_part(bool reset);
+unsigned int check_line_search(bool reset);
 cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,
                          cudaStream_t st);
 

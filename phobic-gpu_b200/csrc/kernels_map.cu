@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
             uint32_t slot[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; u++)
-                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&cnt[gp[u]], 1u);
+                if (gp[u] != 0xFFFFFFFFu) slot[u] = PHB_CHECK(gp[u] < a.M) ? atomicAdd(&cnt[gp[u]], 1u) : 0u;
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
         } else {
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
-                if (gp[u] == 0xFFFFFFFFu) continue;
+                if (gp[u] == 0xFFFFFFFFu || !PHB_CHECK(gp[u] < a.M)) continue;
                 atomicAdd(&cnt[gp[u]], 1u);
                 if (KIND == PHOBIC_KEYS_STRINGS)
                     a.mapped[g0 + (uint64_t)u * kChunkThreads] = make_uint4(gp[u], b[u], l1[u], l2[u]);
@@ -207,6 +207,8 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
         for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) a.counts[(size_t)g * a.stride + c] = cnt[g];
     }
 }
+
+unsigned int check_line_map(bool reset) { return read_check_line(reset); }
 
 static size_t chunk_smem(uint64_t partitions) { return 4 * ((size_t)kFulcrums + (size_t)partitions); }
 

@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
                 rec[j] = make_uint4(k.lower1, k.lower2, sc.part_base + partition_of(k.partitioner, sc.partitions),
                                     bucket_of(k.bucketer, sf));
             }
-            rank[j] = atomicAdd(&hist[rec[j].z >> p.wshift], 1u);
+            if (PHB_CHECK((rec[j].z >> p.wshift) < p.nbins)) rank[j] = atomicAdd(&hist[rec[j].z >> p.wshift], 1u);
         }
         __syncthreads();
         block_exclusive_scan(hist, loff, p.nbins, warp_sums);
@@ -135,11 +135,13 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
             if (hist[b]) gbase[b] = atomicAdd(&p.bincur[b], hist[b]) - loff[b];
 #pragma unroll
         for (int j = 0; j < kPartItems; j++)
-            if (rank[j] != 0xFFFFFFFFu) stage[loff[rec[j].z >> p.wshift] + rank[j]] = rec[j];
+            if (rank[j] != 0xFFFFFFFFu && PHB_CHECK(loff[rec[j].z >> p.wshift] + rank[j] < (uint32_t)kPartTile))
+                stage[loff[rec[j].z >> p.wshift] + rank[j]] = rec[j];
         __syncthreads();
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
-            p.inter[gbase[r.z >> p.wshift] + q] = r;
+            const uint64_t dst = (uint64_t)gbase[r.z >> p.wshift] + q;
+            if (PHB_CHECK(dst < a.total_keys)) p.inter[dst] = r;
         }
         __syncthreads();
     }
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
                 const uint32_t q = j * kPartThreads + threadIdx.x;
                 if (q >= count) continue;
                 const uint32_t dst = atomicAdd(&p.pcur[rec[j].z], 1u);
+                if (!PHB_CHECK(dst < total)) continue;
                 lowers[dst] = make_uint2(rec[j].x, rec[j].y);
                 bkt[dst] = (uint16_t)rec[j].w;
             }
@@ -199,7 +202,8 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
         block_exclusive_scan(hist, base, range, warp_sums);  // base = local offsets for now
 #pragma unroll
         for (int j = 0; j < kPartItems; j++)
-            if (rank[j] != 0xFFFFFFFFu) stage[base[rec[j].z - gmin] + rank[j]] = rec[j];
+            if (rank[j] != 0xFFFFFFFFu && PHB_CHECK(base[rec[j].z - gmin] + rank[j] < (uint32_t)kPartTile))
+                stage[base[rec[j].z - gmin] + rank[j]] = rec[j];
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < range; i += blockDim.x)
             if (hist[i]) base[i] = atomicAdd(&p.pcur[gmin + i], hist[i]) - base[i];
@@ -207,12 +211,15 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
             const uint32_t dst = base[r.z - gmin] + q;
+            if (!PHB_CHECK(dst < total)) continue;
             lowers[dst] = make_uint2(r.x, r.y);
             bkt[dst] = (uint16_t)r.w;
         }
         __syncthreads();
     }
 }
+
+unsigned int check_line_part(bool reset) { return read_check_line(reset); }
 
 uint32_t part_wshift(uint64_t partitions) {
     uint32_t w = 0;

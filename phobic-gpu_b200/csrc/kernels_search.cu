@@ -84,6 +84,7 @@ struct WarpSmem {
     uint32_t *cnt32;                    // packed u16 pairs
     uint32_t *sched;
     uint32_t *occ;
+    uint32_t occ_lo, occ_hi;  // shared-space byte bounds of the bitmap (checked build)
 };
 
 __device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap) {
@@ -96,6 +97,8 @@ __device__ __forceinline__ WarpSmem carve(uint32_t *w, uint32_t B, uint32_t cap)
     m.cnt32 = w + union_words(B, cap);
     m.sched = m.cnt32 + half_words(B);
     m.occ = m.sched + B;
+    m.occ_lo = (uint32_t)__cvta_generic_to_shared(m.occ);
+    m.occ_hi = m.occ_lo + 4 * bitmap_words(cap);
     return m;
 }
 
@@ -132,6 +135,12 @@ __device__ __forceinline__ uint32_t lds32_next(uint32_t addr) {
     asm volatile("ld.shared.u32 %0, [%1+4];" : "=r"(v) : "r"(addr));
     return v;
 }
+// The 32-bit window starting `sh` bits into the bitmap word at byte address `addr`;
+// in the checked build the two words must lie inside [lo, hi).
+__device__ __forceinline__ uint32_t window_at(uint32_t addr, uint32_t sh, uint32_t lo, uint32_t hi) {
+    if (!PHB_CHECK(addr >= lo && addr + 8 <= hi)) return kFullMask;
+    return __funnelshift_r(lds32(addr), lds32_next(addr), sh);
+}
 __device__ __forceinline__ uint4 lds128(uint32_t addr) {
     uint4 v;
     asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr));
@@ -150,7 +159,7 @@ __device__ __forceinline__ uint32_t unpack_slot(uint32_t v) { return ((v >> 7) <
 // 128-bit load.  A round stops early once every lane's window holds an occupied
 // slot.  The bitmap is addressed through 32-bit shared-memory addresses.
 __device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, const uint32_t *hs, uint32_t s,
-                                                      uint32_t ps, int lane) {
+                                                      uint32_t ps, int lane, uint32_t lo, uint32_t hi) {
     const uint32_t occ_sa = (uint32_t)__cvta_generic_to_shared(occ);
     const uint32_t hs_sa = (uint32_t)__cvta_generic_to_shared(hs);
     for (uint32_t w0 = 0; w0 < ps; w0 += 1024) {
@@ -162,8 +171,8 @@ __device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, const
             const uint4 v = lds128(hs_sa + 4 * i);
             const uint32_t a0 = base + (v.x >> 5), a1 = base + (v.y >> 5);
             const uint32_t a2 = base + (v.z >> 5), a3 = base + (v.w >> 5);
-            bad |= __funnelshift_r(lds32(a0), lds32_next(a0), v.x) | __funnelshift_r(lds32(a1), lds32_next(a1), v.y);
-            bad |= __funnelshift_r(lds32(a2), lds32_next(a2), v.z) | __funnelshift_r(lds32(a3), lds32_next(a3), v.w);
+            bad |= window_at(a0, v.x, lo, hi) | window_at(a1, v.y, lo, hi);
+            bad |= window_at(a2, v.z, lo, hi) | window_at(a3, v.w, lo, hi);
             if (__all_sync(kFullMask, bad == kFullMask)) break;
         }
         uint32_t valid = ~bad;
@@ -184,7 +193,8 @@ __device__ __forceinline__ uint32_t first_free_offset(const uint32_t *occ, const
 // window is still open after the first four keys.  Dead lanes (w >= ps) read at
 // offset 0, inside the bitmap, and count as fully occupied.
 template <int K>
-__device__ __forceinline__ uint32_t first_free_offset_reg(const uint32_t *occ, uint32_t hp, uint32_t ps, int lane) {
+__device__ __forceinline__ uint32_t first_free_offset_reg(const uint32_t *occ, uint32_t hp, uint32_t ps, int lane,
+                                                          uint32_t blo, uint32_t bhi) {
     const uint32_t occ_sa = (uint32_t)__cvta_generic_to_shared(occ);
     uint32_t v[K], hb[K];
 #pragma unroll
@@ -198,12 +208,11 @@ __device__ __forceinline__ uint32_t first_free_offset_reg(const uint32_t *occ, u
         const uint32_t lo = live ? (w >> 3) : 0u;
         uint32_t bad = 0;
 #pragma unroll
-        for (int i = 0; i < (K < 4 ? K : 4); i++) bad |= __funnelshift_r(lds32(hb[i] + lo), lds32_next(hb[i] + lo), v[i]);
+        for (int i = 0; i < (K < 4 ? K : 4); i++) bad |= window_at(hb[i] + lo, v[i], blo, bhi);
         if (K == 8) {
             if (!__all_sync(kFullMask, bad == kFullMask || !live)) {
 #pragma unroll
-                for (int i = 4; i < K; i++)
-                    bad |= __funnelshift_r(lds32(hb[i] + lo), lds32_next(hb[i] + lo), v[i]);
+                for (int i = 4; i < K; i++) bad |= window_at(hb[i] + lo, v[i], blo, bhi);
             }
         }
         uint32_t valid = live ? ~bad : 0u;
@@ -228,18 +237,22 @@ __device__ __forceinline__ uint32_t lds32_at(uint32_t addr) {
 // some lane's window holds a free offset, which is written to *o.
 template <int K, int R>
 __device__ __forceinline__ bool scan_round(const uint32_t (&hb)[K], const uint32_t (&v)[K], uint32_t ps, int lane,
-                                           uint32_t *o) {
+                                           uint32_t *o, uint32_t blo, uint32_t bhi) {
     // Offsets of this lane's window below ps, as a mask (clamped funnel shift: n >= 32 gives all ones).
     const int n = (int)ps - (int)(1024 * R) - 32 * lane;
     uint32_t bad = ~__funnelshift_lc(kFullMask, 0u, (uint32_t)max(n, 0));
 #pragma unroll
     for (int i = 0; i < (K < 4 ? K : 4); i++)
-        bad |= __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i]);
+        bad |= PHB_CHECK(hb[i] + 128 * R >= blo && hb[i] + 128 * R + 8 <= bhi)
+                   ? __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i])
+                   : kFullMask;
     if (K == 8) {
         if (!__all_sync(kFullMask, bad == kFullMask)) {
 #pragma unroll
             for (int i = 4; i < K; i++)
-                bad |= __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i]);
+                bad |= PHB_CHECK(hb[i] + 128 * R >= blo && hb[i] + 128 * R + 8 <= bhi)
+                           ? __funnelshift_r(lds32_at<128 * R>(hb[i]), lds32_at<128 * R + 4>(hb[i]), v[i])
+                           : kFullMask;
         }
     }
     const uint32_t ball = __ballot_sync(kFullMask, bad != kFullMask);
@@ -255,7 +268,7 @@ __device__ __forceinline__ bool scan_round(const uint32_t (&hb)[K], const uint32
 // read inside the padded bitmap (bitmap_words) and are masked.
 template <int K>
 __device__ __forceinline__ uint32_t first_free_offset_unr(const uint32_t *occ, uint32_t hp, uint32_t ps,
-                                                          uint32_t rounds, int lane) {
+                                                          uint32_t rounds, int lane, uint32_t blo, uint32_t bhi) {
     const uint32_t lane_sa = (uint32_t)__cvta_generic_to_shared(occ) + 4u * lane;
     uint32_t v[K], hb[K];
 #pragma unroll
@@ -264,9 +277,9 @@ __device__ __forceinline__ uint32_t first_free_offset_unr(const uint32_t *occ, u
         hb[i] = lane_sa + (v[i] >> 5);
     }
     uint32_t o = kNone;
-    if (scan_round<K, 0>(hb, v, ps, lane, &o)) return o;
-    if (rounds > 1 && scan_round<K, 1>(hb, v, ps, lane, &o)) return o;
-    if (rounds > 2 && scan_round<K, 2>(hb, v, ps, lane, &o)) return o;
+    if (scan_round<K, 0>(hb, v, ps, lane, &o, blo, bhi)) return o;
+    if (rounds > 1 && scan_round<K, 1>(hb, v, ps, lane, &o, blo, bhi)) return o;
+    if (rounds > 2 && scan_round<K, 2>(hb, v, ps, lane, &o, blo, bhi)) return o;
     return kNone;
 }
 
@@ -299,20 +312,21 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
         if (s <= 8 && rounds <= 3) {
             // Two unrolled variants only: a smaller hot loop (fewer instruction-cache
             // misses) outweighs the repeated slot of buckets of one or two keys.
-            if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane);
-            else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane);
-        } else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane);
-        else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane);
+            if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
+            else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
+        } else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
+        else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
         else {
             if (lane < (int)padded) ws.hs[lane] = hp;
             __syncwarp();
-            o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+            o = first_free_offset(ws.occ, ws.hs, s, ps, lane, ws.occ_lo, ws.occ_hi);
             __syncwarp();
         }
         if (o == kNone) continue;
         if (mine) {
             uint32_t q = h + o;
-            mark(ws.occ, q >= ps ? q - ps : q, ps);
+            q = q >= ps ? q - ps : q;
+            if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
         }
         __syncwarp();
         *pilot = o + ps * k;
@@ -346,7 +360,7 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
                 const uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
                 ws.hs[i] = pack_slot(h);
                 const uint32_t bit = 1u << (h & 31);
-                d = (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+                d = PHB_CHECK(h < ps) && (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
             }
             dup = __any_sync(kFullMask, d);
             done = c0 + 32;
@@ -356,12 +370,13 @@ __device__ __forceinline__ uint32_t place_large(const WarpSmem &ws, const uint2 
         if (dup) continue;
         if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
         __syncwarp();
-        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane, ws.occ_lo, ws.occ_hi);
         __syncwarp();
         if (o == kNone) continue;
         for (uint32_t i = lane; i < s; i += 32) {
             uint32_t q = unpack_slot(ws.hs[i]) + o;
-            mark(ws.occ, q >= ps ? q - ps : q, ps);
+            q = q >= ps ? q - ps : q;
+            if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
         }
         __syncwarp();
         *pilot = o + ps * k;
@@ -407,7 +422,7 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
                     const uint32_t h = fm.mod(pilot_hash(key[c].x, key[c].y, k));
                     ws.hs[i] = pack_slot(h);
                     const uint32_t bit = 1u << (h & 31);
-                    d = (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+                    d = PHB_CHECK(h < ps) && (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
                 }
                 dup = __any_sync(kFullMask, d);
                 done = c + 1;
@@ -422,7 +437,7 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
         if (dup) continue;
         if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
         __syncwarp();
-        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane);
+        const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane, ws.occ_lo, ws.occ_hi);
         __syncwarp();
         if (o == kNone) continue;
 #pragma unroll
@@ -430,7 +445,8 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
             const uint32_t i = 32 * c + lane;
             if (i < s) {
                 uint32_t q = unpack_slot(ws.hs[i]) + o;
-                mark(ws.occ, q >= ps ? q - ps : q, ps);
+                q = q >= ps ? q - ps : q;
+                if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
             }
         }
         __syncwarp();
@@ -447,6 +463,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     const uint32_t base = a.G[(size_t)g * a.gstride];
     const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
     if (ps > a.cap) return PHOBIC_OK;  // reported by the size check
+    if (!PHB_CHECK(base + ps <= a.G[(size_t)a.M * a.gstride])) return PHOBIC_OK;
     const uint32_t ow = bitmap_words(a.cap);
     uint32_t *pil = d.pilots + p;
     const size_t pstride = d.partitions;
@@ -459,7 +476,10 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     // Bucket sizes of this partition (bucket_sizes.comp:21-35).
     const uint16_t *bk = a.bkt + base;
 #pragma unroll 4
-    for (uint32_t i = lane; i < ps; i += 32) half_add(ws.cnt32, bk[i]);
+    for (uint32_t i = lane; i < ps; i += 32) {
+        const uint32_t b = bk[i];
+        if (PHB_CHECK(b < B)) half_add(ws.cnt32, b);
+    }
     __syncwarp();
 
     // Size histogram in bins 256 - size (sort_sum.comp:56-58,166-170); empty buckets get pilot 0.
@@ -468,7 +488,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         uint32_t s = half_get(ws.cnt32, b);
         if (a.debug_sizes) a.debug_sizes[(size_t)g * B + b] = s;
         if (s > kMaxBucket) over = true;
-        else if (s) half_add(ws.binPos, kBins - s);
+        else if (s && PHB_CHECK(s <= kBins)) half_add(ws.binPos, kBins - s);
         else pil[(size_t)b * pstride] = 0;
     }
     if (__any_sync(kFullMask, over)) return PHOBIC_ERR_BUCKET_OVERFLOW;
@@ -509,8 +529,10 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         const uint32_t bin = kBins - s;
         if (s) {
             const uint32_t j = half_get(ws.binPos, bin) + r, st = half_get(ws.binKey, bin) + r * s;
-            ws.sched[j] = st | ((uint32_t)bi << 16);
-            cur16[bi] = (uint16_t)st;
+            if (PHB_CHECK(j < B && st + s <= ps)) {
+                ws.sched[j] = st | ((uint32_t)bi << 16);
+                cur16[bi] = (uint16_t)st;
+            }
         }
         __syncwarp();
         if (s && lane == __ffs(peers) - 1) {
@@ -525,8 +547,10 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     uint2 *so = a.sorted + base;
 #pragma unroll 4
     for (uint32_t i = lane; i < ps; i += 32) {
-        uint32_t b = bk[i];
-        so[half_add(ws.cur32, b)] = lo[i];
+        const uint32_t b = bk[i];
+        if (!PHB_CHECK(b < B)) continue;
+        const uint32_t pos = half_add(ws.cur32, b);
+        if (PHB_CHECK(pos < ps)) so[pos] = lo[i];
     }
     __threadfence_block();
     __syncwarp();
@@ -556,12 +580,14 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
                                  : s <= 64  ? place_large_reg<2>(ws, so + st, s, ps, fm, k_lim, lane, &pilot)
                                             : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
         if (st_code != PHOBIC_OK) return st_code;
-        if (lane == 0) pil[(size_t)b * pstride] = pilot;
+        if (lane == 0 && PHB_CHECK(b < B)) pil[(size_t)b * pstride] = pilot;
     }
     return PHOBIC_OK;
 }
 
 }  // namespace
+
+unsigned int check_line_search(bool reset) { return read_check_line(reset); }
 
 size_t search_warp_smem(uint32_t buckets, uint32_t cap) { return 4 * warp_words(buckets, cap); }
 

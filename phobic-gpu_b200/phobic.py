@@ -22,7 +22,9 @@ from pathlib import Path
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "lib" / "libphobic_b200.so"
+# PHOBIC_LIBRARY=checked selects the bounds-checked build of the same library.
+LIB_PATH = PKG / "lib" / ("libphobic_b200_checked.so" if os.environ.get("PHOBIC_LIBRARY") == "checked"
+                          else "libphobic_b200.so")
 FULCRUMS = 2048
 
 OK, ERR_INVALID, ERR_OOM, ERR_BUCKET_OVERFLOW, ERR_PARTITION_OVERFLOW = 0, 1, 2, 3, 4
@@ -136,6 +138,7 @@ def _lib() -> C.CDLL:
         "phobic_verify": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_debug_build": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P, P]),
         "phobic_debug_stalled_wait": (I32, [P, U32, C.POINTER(I32)]),
+        "phobic_debug_checks": (I32, [P, C.POINTER(I32), C.POINTER(U32), I32]),
         "phobic_encode": (I32, [I32, I32, P, P, U32, C.POINTER(Params), C.c_float, P, C.c_size_t,
                                 C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
         "phobic_encode_gpu": (I32, [P, I32, I32, C.POINTER(Result), U32, C.POINTER(Params), P, C.c_size_t, I32,
@@ -343,6 +346,14 @@ class Context:
     def set_memory_limit(self, nbytes: int) -> None:
         """Cap the device memory of this context's build pool (0 = no cap)."""
         check(_lib().phobic_ctx_set_memory_limit(self.handle, nbytes), self)
+
+    def checks(self, reset: bool = False) -> tuple[bool, list[int]]:
+        """(checked library?, source lines of the first failed bounds check in the
+        key-mapping, partition and search kernels; 0 = none)."""
+        compiled = C.c_int32()
+        lines = (U32 * 3)()
+        check(_lib().phobic_debug_checks(self.handle, C.byref(compiled), lines, int(reset)), self)
+        return bool(compiled.value), list(lines)
 
     def stalled_wait(self, wait_ms: int) -> int:
         """Status recorded by a kernel whose bounded wait on a never-set flag ran out."""

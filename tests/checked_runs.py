@@ -1,0 +1,59 @@
+"""Parity builds on the bounds-checked library (run by test_gpu_checked.py in a
+process of its own, with PHOBIC_LIBRARY=checked): every build must match the
+oracle bit for bit and no bounds check may fail."""
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+sys.path.insert(0, str(ROOT / "phobic-gpu_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
+
+import numpy as np  # noqa: E402
+
+import keygen  # noqa: E402
+import oracle_lib as O  # noqa: E402
+import phobic  # noqa: E402
+
+
+def main() -> int:
+    assert phobic.LIB_PATH.name == "libphobic_b200_checked.so", phobic.LIB_PATH
+    with phobic.Context(0) as ctx:
+        compiled, lines = ctx.checks(reset=True)
+        assert compiled, "not the checked library"
+        cases = [(7.0, 2500, n) for n in (1, 2, 31, 2047, 2049, 10_000, 300_000)]
+        cases += [(5.0, 2048, 200_000), (4.5, 2500, 100_000), (3.0, 1024, 60_000), (6.0, 4096, 60_000),
+                  (2.0, 256, 40_000), (8.0, 8192, 60_000), (8.0, 8192, 50_000)]
+        for lam, P, n in cases:
+            cfg = phobic.MPHFconfig(lam, P)
+            keys = keygen.splitmix64(90 + n, n)
+            want = O.build(O.hash_keys(keys, "u64"), P, cfg.bucketCountPerPartition, cfg.getFulcs())
+            if want["status"] != 0:  # e.g. a bucket above 256 keys: the same error status
+                try:
+                    ctx.build(keys, cfg)
+                    raise AssertionError(f"no error for {(lam, P, n)}")
+                except phobic.PhobicError as e:
+                    assert e.status == want["status"], (lam, P, n, e.status, want["status"])
+                continue
+            got = ctx.build(keys, cfg)
+            assert np.array_equal(got.pilots, want["pilots"]), (lam, P, n)
+            assert np.array_equal(got.partition_offsets, want["offsets"]), (lam, P, n)
+        strs = [bytes(keygen.splitmix64(7, 1).view(np.uint8)[: i % 8]) * 5 + b"%d" % i for i in range(30_000)]
+        offs = np.zeros(len(strs) + 1, np.uint64)
+        np.cumsum([len(x) for x in strs], out=offs[1:])
+        data = np.frombuffer(b"".join(strs), np.uint8)
+        cfg = phobic.MPHFconfig(6.0, 2048)
+        got = ctx.build((data, offs), cfg)
+        want = O.build(O.hash_keys((data, offs), "strings"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs())
+        assert np.array_equal(got.pilots, want["pilots"])
+        sets = [keygen.splitmix64(200 + i, 1000 * (i + 1)) for i in range(12)]
+        res, st = phobic.build_batch(ctx, sets, cfg)
+        for ks, r in zip(sets, res):
+            w = O.build(O.hash_keys(ks, "u64"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs())
+            assert np.array_equal(r.pilots, w["pilots"])
+        compiled, lines = ctx.checks()
+        print("checked builds:", len(cases) + 2, "failed check lines (map, partition, search):", lines)
+        return 0 if lines == [0, 0, 0] else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())
