@@ -136,6 +136,26 @@ def test_bijection_at_ten_million(phobic, ctx):
     assert got.partition_offsets[-1] == len(keys) and (np.diff(got.partition_offsets.astype(np.int64)) >= 0).all()
 
 
+def test_bijection_beyond_two_to_the_31_keys(phobic):
+    """One set of 2.3 billion keys (above 2^31, so a signed 32-bit index anywhere on the
+    path would overflow): the build is a bijection onto [0, n) under the on-device query,
+    and the partition offsets end at n.  About 80 GB of device memory."""
+    torch = pytest.importorskip("torch")
+    n = 2_300_000_000
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    parts, B = cfg.partitions(n), cfg.bucketCountPerPartition
+    keys = keygen.splitmix64_cuda(2, n)
+    with phobic.Context(0) as c:
+        pil = torch.zeros(B * parts, dtype=torch.int32, device="cuda")
+        off = torch.zeros(parts + 1, dtype=torch.int32, device="cuda")
+        c.build(keys, cfg, out=(pil, off))
+        assert c.verify(keys, cfg, phobic.BuildResult(pil, off, parts, B)) == 0
+        last = int(off[-1].item()) & 0xFFFFFFFF
+        assert last == n
+    del keys, pil, off
+    torch.cuda.empty_cache()
+
+
 def test_repeated_builds_are_identical(phobic, ctx):
     keys = keygen.splitmix64(6, 500_000)
     cfg = phobic.MPHFconfig(7.0, 2500)
