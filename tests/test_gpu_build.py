@@ -214,3 +214,32 @@ def test_context_survives_errors(phobic, ctx):
     good = keygen.splitmix64(1, 3000)
     got = ctx.build(good, cfg)
     assert ctx.verify(good, cfg, got) == 0
+
+
+@pytest.mark.parametrize("case", range(24))
+def test_random_configurations_match_oracle(phobic, ctx, case):
+    """A seeded sweep of configurations: lambda in [1.5, 9], partition size 64..6000,
+    0..150 000 keys, any bucketer and constructor, u64 or 16-byte keys.  The GPU result
+    equals the oracle's bit for bit, or both report the same error (an oversized
+    partition or bucket)."""
+    rng = np.random.default_rng(1000 + case)
+    lam = float(np.round(rng.uniform(1.5, 9.0), 2))
+    P = int(rng.choice([64, 100, 256, 777, 1024, 2048, 2500, 3000, 4096, 6000]))
+    n = int(rng.integers(0, 150_000)) if case % 4 else int(rng.integers(0, 300))
+    bucketer, ctor = int(rng.integers(0, 3)), int(rng.integers(0, 2))
+    cfg = phobic.MPHFconfig(lam, P, bucketer, bool(ctor))
+    if case % 3 == 2:
+        keys = keygen.splitmix64(3000 + case, 2 * n).reshape(n, 2)
+        keys4, kind = O.hash_keys(keys, "pairs"), phobic.KEYS_BYTES16
+    else:
+        keys = keygen.splitmix64(3000 + case, n)
+        keys4, kind = O.hash_keys(keys, "u64"), phobic.KEYS_U64
+    want = oracle_build(keys4, cfg)
+    if want["status"] != 0:
+        with pytest.raises(phobic.PhobicError) as e:
+            ctx.build(keys, cfg, kind=kind)
+        assert e.value.status == want["status"], (lam, P, n, bucketer, ctor)
+        return
+    got = ctx.build(keys, cfg, kind=kind)
+    assert (got.partition_offsets == want["offsets"]).all(), (lam, P, n, bucketer, ctor)
+    assert (got.pilots == want["pilots"]).all(), (lam, P, n, bucketer, ctor)
