@@ -101,7 +101,8 @@ struct PartArgs {
     uint32_t wshift;    // coarse bin = partition >> wshift
     uint32_t nbins;     // ceil(M / 2^wshift) <= kMaxBins
 };
-// Smallest shift giving at most kTargetBins coarse bins.
+// Smallest shift giving at most kTargetBins coarse bins, lowered (up to kMaxBins bins)
+// until two bins span at most kLocalRange partitions.
 uint32_t part_wshift(uint64_t partitions);
 
 struct ScanArgs {

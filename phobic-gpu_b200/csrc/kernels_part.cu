@@ -224,6 +224,10 @@ unsigned int check_line_part(bool reset) { return read_check_line(reset); }
 uint32_t part_wshift(uint64_t partitions) {
     uint32_t w = 0;
     while (((partitions + (1ull << w) - 1) >> w) > kTargetBins) w++;
+    // A pass-2 tile spans at most two bins; keep that within kLocalRange partition ids
+    // (else pass 2 places its records one atomic at a time) as long as the bins fit
+    // kMaxBins.
+    while ((2ull << w) > kLocalRange && w > 0 && ((partitions + (1ull << (w - 1)) - 1) >> (w - 1)) <= kMaxBins) w--;
     return w;
 }
 
