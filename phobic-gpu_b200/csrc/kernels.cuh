@@ -25,7 +25,11 @@ constexpr int kMapThreads = 256;
 constexpr int kChunkThreads = 1024;
 constexpr uint32_t kChunkCtas = 148;                 // one CTA per SM of a B200
 constexpr uint64_t kChunkMinKeys = 16384;            // smallest chunk worth a CTA
-constexpr uint32_t kChunkMaxPartitions = 52 * 1024;  // shared-memory counters per CTA
+constexpr uint32_t kChunkMaxPartitions = 52 * 1024;  // 32-bit shared-memory counters per CTA
+// Counting only (K1): above kChunkMaxPartitions the counters are packed two to a
+// 32-bit word.  A 16-bit counter that wraps is caught from the atomic's return value
+// and the 65536 keys it lost are added to the chunk's count in global memory.
+constexpr uint32_t kChunkNarrowMaxPartitions = 104 * 1024;
 constexpr int kScanThreads = 512;
 constexpr int kScanItems = 8;  // entries per thread: one tile = 4096 entries
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -65,6 +69,7 @@ struct MapPlan {
     uint32_t stride;  // count-matrix entries per partition (chunks, or 1)
     uint32_t grid;
     uint64_t chunk;   // keys per CTA (chunked plan)
+    bool narrow;      // chunked with 16-bit counters: K1 counting only, launch_scatter refuses it
 };
 MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count);
 

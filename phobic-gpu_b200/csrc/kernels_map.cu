@@ -13,7 +13,8 @@
 //   chunked  CTA c counts (K1) and places (K3) the keys of one contiguous chunk
 //            with a shared-memory counter per partition; the only global traffic
 //            is the streamed keys, one column of the count matrix and the record
-//            stores.  Used while all partitions' counters fit in shared memory.
+//            stores.  Used while all partitions' counters fit in shared memory,
+//            32-bit up to 52K partitions, packed 16-bit (counting) up to 104K.
 //   global   one counter per partition in global memory, a reduction per key in
 //            K1 and an atomic add per key in K3 (builds with more partitions).
 #include "kernels.cuh"
@@ -115,20 +116,39 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
     if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
 }
 
+// A 16-bit counter of the packed plan went from 0xFFFF to 0 in the add that
+// returned `old`: credit the 65536 keys to column c of the count matrix.  The
+// half-word arithmetic is exact because each half only ever steps by one: a low
+// half (even partition g) that wraps carries one into the high half (g + 1),
+// which is taken back here, and if that carry wrapped the high half too, the
+// high half's 65536 is credited as well.  An odd partition's wrap carries out of
+// the word.  Rare by construction: it takes 65536 keys of one partition in one
+// chunk, and the build then fails its size check (partitions hold <= 65535 keys).
+static __device__ __forceinline__ void credit_wrap(const MapArgs &a, uint32_t c, uint32_t g, uint32_t old, uint32_t *wrapped) {
+    *wrapped = 1u;
+    atomicAdd(&a.counts[(size_t)g * a.stride + c], 65536u);
+    if ((g & 1u) == 0 && g + 1 < a.M)
+        atomicAdd(&a.counts[(size_t)(g + 1) * a.stride + c], (old >> 16) == 0xFFFFu ? 65535u : 0xFFFFFFFFu);
+}
+
 // Chunked plan: CTA c owns keys [c * chunk, (c + 1) * chunk).  K1 counts them per
 // partition in shared memory and writes column c of the count matrix; K3 loads
 // column c of its exclusive scan as cursors and hands out slots with
-// shared-memory atomics.
-template <int KIND, bool SCATTER>
+// shared-memory atomics.  NARROW (K1 only) packs two 16-bit counters per word.
+template <int KIND, bool SCATTER, bool NARROW>
 __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
+    static_assert(!(SCATTER && NARROW), "slots need 32-bit cursors");
     extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t wrapped;       // a 16-bit counter wrapped in this CTA
     uint32_t *sf = smem;               // [kFulcrums]
-    uint32_t *cnt = smem + kFulcrums;  // [M]
+    uint32_t *cnt = smem + kFulcrums;  // [M], or [(M + 1) / 2] packed
     constexpr bool kReadMapped = SCATTER && KIND == PHOBIC_KEYS_STRINGS;
     const uint32_t c = blockIdx.x;
     if (!kReadMapped)
         for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
-    for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) cnt[g] = SCATTER ? a.counts[(size_t)g * a.stride + c] : 0u;
+    const uint32_t words = NARROW ? (a.M + 1) / 2 : a.M;
+    for (uint32_t g = threadIdx.x; g < words; g += blockDim.x) cnt[g] = SCATTER ? a.counts[(size_t)g * a.stride + c] : 0u;
+    if (threadIdx.x == 0) wrapped = 0u;
     __syncthreads();
 
     const uint64_t lo = (uint64_t)c * a.chunk;
@@ -191,6 +211,20 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
                 a.lowers[slot[u]] = make_uint2(l1[u], l2[u]);
                 a.bkt[slot[u]] = (uint16_t)b[u];
             }
+        } else if constexpr (NARROW) {
+            uint32_t old[kUnroll];
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++) {
+                old[u] = 0u;
+                if (gp[u] == 0xFFFFFFFFu || !PHB_CHECK(gp[u] < a.M)) continue;
+                old[u] = atomicAdd(&cnt[gp[u] >> 1], 1u << ((gp[u] & 1u) << 4));
+                if (KIND == PHOBIC_KEYS_STRINGS)
+                    a.mapped[g0 + (uint64_t)u * kChunkThreads] = make_uint4(gp[u], b[u], l1[u], l2[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < kUnroll; u++)
+                if (gp[u] < a.M && ((old[u] >> ((gp[u] & 1u) << 4)) & 0xFFFFu) == 0xFFFFu)
+                    credit_wrap(a, c, gp[u], old[u], &wrapped);
         } else {
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
@@ -204,23 +238,38 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
     if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
     if (!SCATTER) {
         __syncthreads();
-        for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) a.counts[(size_t)g * a.stride + c] = cnt[g];
+        if (NARROW) {
+            // After a wrap the column already holds the credited 65536s: add to it.
+            const bool add = wrapped != 0u;
+            for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) {
+                const uint32_t v = (cnt[g >> 1] >> ((g & 1u) << 4)) & 0xFFFFu;
+                if (add)
+                    atomicAdd(&a.counts[(size_t)g * a.stride + c], v);
+                else
+                    a.counts[(size_t)g * a.stride + c] = v;
+            }
+        } else {
+            for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) a.counts[(size_t)g * a.stride + c] = cnt[g];
+        }
     }
 }
 
 unsigned int check_line_map(bool reset) { return read_check_line(reset); }
 
-static size_t chunk_smem(uint64_t partitions) { return 4 * ((size_t)kFulcrums + (size_t)partitions); }
+static size_t chunk_smem(uint64_t partitions, bool narrow) {
+    return 4 * ((size_t)kFulcrums + (size_t)(narrow ? (partitions + 1) / 2 : partitions));
+}
 
 MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count) {
     MapPlan p{};
-    if (partitions <= kChunkMaxPartitions && total_keys > 0) {
+    if (partitions <= kChunkNarrowMaxPartitions && total_keys > 0) {
         uint64_t ctas = (total_keys + kChunkMinKeys - 1) / kChunkMinKeys;
         if (ctas > kChunkCtas) ctas = kChunkCtas;
         p.chunked = true;
         p.stride = (uint32_t)ctas;
         p.grid = (uint32_t)ctas;
         p.chunk = (total_keys + ctas - 1) / ctas;
+        p.narrow = partitions > kChunkMaxPartitions;
     } else {
         p.chunked = false;
         p.stride = 1;
@@ -232,14 +281,25 @@ MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count) {
     return p;
 }
 
+template <int KIND, bool SCATTER, bool NARROW>
+static cudaError_t launch_chunk(const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    const size_t smem = chunk_smem(a.M, NARROW);
+    cudaError_t e = cudaFuncSetAttribute(k_chunk<KIND, SCATTER, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    k_chunk<KIND, SCATTER, NARROW><<<plan.grid, kChunkThreads, smem, st>>>(a);
+    return cudaSuccess;
+}
+
 template <bool SCATTER, int KIND>
 static cudaError_t launch_kind(const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
     if (plan.chunked) {
-        const size_t smem = chunk_smem(a.M);
-        cudaError_t e = cudaFuncSetAttribute(k_chunk<KIND, SCATTER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e;
+        if constexpr (SCATTER)
+            e = plan.narrow ? cudaErrorInvalidValue : launch_chunk<KIND, true, false>(a, plan, st);
+        else
+            e = plan.narrow ? launch_chunk<KIND, false, true>(a, plan, st) : launch_chunk<KIND, false, false>(a, plan, st);
         if (e != cudaSuccess) return e;
-        k_chunk<KIND, SCATTER><<<plan.grid, kChunkThreads, smem, st>>>(a);
     } else {
         k_map<KIND, SCATTER><<<plan.grid, kMapThreads, 0, st>>>(a);
     }

@@ -23,7 +23,8 @@ def main() -> int:
         cases = [(7.0, 2500, n) for n in (1, 2, 31, 2047, 2049, 10_000, 300_000)]
         cases += [(5.0, 2048, 200_000), (4.5, 2500, 100_000), (3.0, 1024, 60_000), (6.0, 4096, 60_000),
                   (2.0, 256, 40_000), (8.0, 8192, 60_000), (8.0, 8192, 50_000), (3.63, 64, 84_498),
-                  (5.95, 100, 68_243), (4.03, 100, 90_128), (1.5, 777, 137_762)]
+                  (5.95, 100, 68_243), (4.03, 100, 90_128), (1.5, 777, 137_762),
+                  (5.0, 200, 12_000_000)]  # 60 000 partitions: packed 16-bit counters in K1
         for lam, P, n in cases:
             cfg = phobic.MPHFconfig(lam, P)
             keys = keygen.splitmix64(90 + n, n)

@@ -243,3 +243,92 @@ def test_random_configurations_match_oracle(phobic, ctx, case):
     got = ctx.build(keys, cfg, kind=kind)
     assert (got.partition_offsets == want["offsets"]).all(), (lam, P, n, bucketer, ctor)
     assert (got.pilots == want["pilots"]).all(), (lam, P, n, bucketer, ctor)
+
+
+# ------------------------------------------------------------------ 52K-104K partitions: packed 16-bit counters in K1
+
+def chunk_of_plan(n):
+    """Keys per CTA of K1's chunked plan for an n-key build (148 chunks of >= 16384 keys)."""
+    ctas = min(-(-n // 16384), 148)
+    return -(-n // ctas)
+
+
+def partitioner_for(p, M):
+    """The smallest partitioner word that maps to partition p of M (partition = (x * M) >> 32)."""
+    return (p * (1 << 32) + M - 1) // M
+
+
+def random_keys4(seed, n):
+    return np.random.default_rng(seed).integers(0, 1 << 32, size=(n, 4), dtype=np.uint64).astype(np.uint32)
+
+
+@pytest.mark.parametrize("kind", ["u64", "pairs"])
+def test_packed_counter_builds_match_oracle(phobic, ctx, kind):
+    """60 000 partitions of 200 keys: K1 counts in packed 16-bit shared-memory counters;
+    keys, bucket sizes, offsets and pilots equal the oracle's."""
+    n = 12_000_000
+    if kind == "u64":
+        keys, k = keygen.splitmix64(41, n), phobic.KEYS_U64
+    else:
+        keys, k = keygen.splitmix64(42, 2 * n).reshape(n, 2), phobic.KEYS_BYTES16
+    assert 52 * 1024 < phobic.MPHFconfig(5.0, 200).partitions(n) <= 104 * 1024
+    check_against_oracle(phobic, ctx, keys, k, 5.0, 200)
+
+
+def test_packed_counter_batch_matches_oracle(phobic, ctx):
+    """Eight sets whose 58 000 partitions together take the packed plan."""
+    cfg = phobic.MPHFconfig(6.0, 200)
+    sets = [keygen.splitmix64(700 + i, 400_000 + 300_000 * i) for i in range(8)]
+    assert 52 * 1024 < sum(cfg.partitions(len(s)) for s in sets) <= 104 * 1024
+    res, st = phobic.build_batch(ctx, sets, cfg)
+    for ks, r, s in zip(sets, res, st):
+        w = oracle_build(O.hash_keys(ks, "u64"), cfg)
+        assert s == w["status"]
+        if s == 0:
+            assert (r.pilots == w["pilots"]).all() and (r.partition_offsets == w["offsets"]).all()
+
+
+def test_packed_counter_wrap_reports_lowest_oversized_partition(phobic, ctx):
+    """Two chunks each hold 70 000 keys of one partition, so their 16-bit counters wrap
+    (partition 40 000 in a low half, 30 001 in a high half).  The wraps are credited
+    exactly: the size check reports partition 30 001, as the oracle does."""
+    n, cfg = 12_000_000, phobic.MPHFconfig(5.0, 200)
+    M = cfg.partitions(n)
+    assert 52 * 1024 < M <= 104 * 1024
+    k4 = random_keys4(43, n)
+    chunk = chunk_of_plan(n)
+    assert chunk > 70_000
+    for c, p in ((13, 40_000), (62, 30_001)):
+        k4[c * chunk: c * chunk + 70_000, 0] = partitioner_for(p, M)
+    want = oracle_build(k4, cfg)
+    assert want["status"] == phobic.ERR_PARTITION_OVERFLOW and want["stats"].err_partition == 30_001
+    with pytest.raises(phobic.PhobicError) as e:
+        ctx.build(k4, cfg, kind=phobic.KEYS_PREHASHED)
+    assert e.value.status == phobic.ERR_PARTITION_OVERFLOW
+    assert "partition 30001)" in str(e.value)
+
+
+def test_packed_counter_carry_into_the_next_set(phobic, ctx):
+    """Set 0's last partition and set 1's first share one packed word.  70 000 keys of
+    the former in one chunk wrap the low half and carry one into the high half; the
+    carry is taken back, so set 1, whose first partition holds exactly the largest
+    allowed size, builds as the oracle builds it."""
+    P = 200
+    cfg = phobic.MPHFconfig(5.0, P)
+    cap = cfg.params.max_partition_size
+    n0, n1 = P * 30_001, P * 30_000
+    M0, M1 = cfg.partitions(n0), cfg.partitions(n1)
+    assert M0 % 2 == 1 and 52 * 1024 < M0 + M1 <= 104 * 1024
+    s0, s1 = random_keys4(44, n0), random_keys4(45, n1)
+    chunk = chunk_of_plan(n0 + n1)
+    s0[13 * chunk: 13 * chunk + 70_000, 0] = partitioner_for(M0 - 1, M0)
+    part1 = (s1[:, 0].astype(np.uint64) * M1) >> 32
+    move = np.flatnonzero(part1 != 0)[: cap - int((part1 == 0).sum())]
+    s1[move, 0] = 0
+    assert int((((s1[:, 0].astype(np.uint64) * M1) >> 32) == 0).sum()) == cap
+    w0, w1 = oracle_build(s0, cfg), oracle_build(s1, cfg)
+    assert w0["status"] == phobic.ERR_PARTITION_OVERFLOW
+    res, st = phobic.build_batch(ctx, [s0, s1], cfg, kind=phobic.KEYS_PREHASHED)
+    assert st == [w0["status"], w1["status"]]
+    if w1["status"] == 0:
+        assert (res[1].pilots == w1["pilots"]).all() and (res[1].partition_offsets == w1["offsets"]).all()
