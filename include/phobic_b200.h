@@ -280,6 +280,14 @@ PHOBIC_API phobic_status phobic_server_poll(phobic_server *srv, uint64_t ticket,
 /* Waits at most timeout_ms for the request (PHOBIC_ERR_TIMEOUT otherwise). */
 PHOBIC_API phobic_status phobic_server_wait(phobic_server *srv, uint64_t ticket, uint32_t timeout_ms, phobic_status *status);
 PHOBIC_API phobic_status phobic_server_drain(phobic_server *srv, uint32_t timeout_ms);
+/* Sizes every stream's device arena to device_bytes and its pinned result stage to
+ * pinned_bytes now, so that requests up to that size allocate nothing while the
+ * streams serve (growing an arena mid-stream frees and reallocates it, which waits
+ * for the whole device).  device_bytes comes from phobic_build_bytes_needed; the
+ * stage holds a batch's results bound for pageable host memory.  PHOBIC_ERR_BUDGET
+ * when streams x device_bytes exceeds the budget, PHOBIC_ERR_BUSY while requests
+ * are pending or in flight. */
+PHOBIC_API phobic_status phobic_server_reserve(phobic_server *srv, uint64_t device_bytes, uint64_t pinned_bytes);
 PHOBIC_API phobic_status phobic_server_stats_get(phobic_server *srv, phobic_server_stats *out);
 PHOBIC_API phobic_status phobic_server_destroy(phobic_server *srv);
 

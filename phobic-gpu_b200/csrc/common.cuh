@@ -16,6 +16,23 @@ constexpr uint32_t kDefaultMaxPilot = 1u << 20;
 constexpr unsigned long long kNoError = ~0ull;
 constexpr unsigned long long kSpinTimeoutNs = 1000000000ull;  // default bound of every spin-wait: 1 s
 
+// Lets `func` take up to the device's opt-in shared memory per block (less its static
+// shared memory) as dynamic shared memory, and checks that `bytes` fit.  The limit is a
+// property of the function shared by all host threads: every caller sets this same
+// value, so a launch from one thread cannot lower it under another thread's launch.
+template <typename F>
+inline cudaError_t allow_dynamic_smem(F *func, size_t bytes) {
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, func);
+    if (e != cudaSuccess) return e;
+    const int limit = optin - (int)fa.sharedSizeBytes;
+    if (limit < 0 || bytes > (size_t)limit) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+}
+
 // Nanosecond clock shared by all SMs, for time-bounded waits.
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;

@@ -88,6 +88,46 @@ void PinnedBuffer::release() {
 
 // ------------------------------------------------------------------ helpers
 
+// True for host memory that is neither pinned nor registered with CUDA.
+static bool is_pageable(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// Stage -> destination copies of finish_sets.  A large copy is split over a few host
+// threads: writing fresh pageable memory is bound by page faults on one core.
+static void copy_out(const std::vector<Worker::HostCopy> &copies, const char *stage) {
+    constexpr size_t kSplitBytes = 4u << 20;
+    constexpr int kParts = 4;
+    for (const auto &c : copies) {
+        char *dst = static_cast<char *>(c.dst);
+        const char *src = stage + c.off;
+        if (c.bytes < kSplitBytes) {
+            std::memcpy(dst, src, c.bytes);
+            continue;
+        }
+        const size_t part = (c.bytes / kParts + 4095) & ~size_t(4095);  // <= c.bytes
+        std::vector<std::thread> helpers;
+        size_t lo = part;  // first byte not handed to a helper
+        for (int i = 1; i < kParts && lo < c.bytes; i++) {
+            const size_t hi = std::min(c.bytes, lo + part);
+            try {
+                helpers.emplace_back([=] { std::memcpy(dst + lo, src + lo, hi - lo); });
+            } catch (...) {  // no thread: this one copies the rest
+                break;
+            }
+            lo = hi;
+        }
+        std::memcpy(dst, src, part);
+        if (lo < c.bytes) std::memcpy(dst + lo, src + lo, c.bytes - lo);
+        for (auto &h : helpers) h.join();
+    }
+}
+
 phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
     if (e == cudaSuccess) return PHOBIC_OK;
     if (err) *err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -144,6 +184,8 @@ void Worker::destroy() {
     }
     arena.release();
     pinned.release();
+    stage.release();
+    pending_copies.clear();
     for (auto &e : ev)
         if (e) cudaEventDestroy(e), e = nullptr;
     if (stream) cudaStreamDestroy(stream), stream = nullptr;
@@ -280,6 +322,26 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     w.pending_err = reinterpret_cast<unsigned long long *>(tab + tab_desc + tab_kb + tab_pb);
     w.pending_sets = nsets;
 
+    // Host results: pinned destinations are copied to directly, pageable ones through the
+    // worker's pinned stage (sized here, before any launch, since growing it reallocates).
+    w.pending_copies.clear();
+    size_t stage_bytes = 0;
+    for (uint32_t i = 0; i < nsets; i++) {
+        if (results[i].on_device) continue;
+        const uint64_t parts = (sets[i].n + P - 1) / P;
+        const std::pair<void *, size_t> arrays[2] = {{results[i].pilots, parts ? 4 * (size_t)B * parts : 0},
+                                                      {results[i].partition_offsets, 4 * ((size_t)parts + 1)}};
+        for (const auto &a : arrays)
+            if (a.second && is_pageable(a.first)) {
+                w.pending_copies.push_back(Worker::HostCopy{a.first, stage_bytes, a.second});
+                stage_bytes += align256(a.second);
+            }
+    }
+    if (stage_bytes && w.stage.reserve(stage_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        w.pending_copies.clear();  // no pinned memory to be had: copy to pageable memory directly
+    }
+
     w.arena.reset();
     PHB_TRY(w.arena.reserve(sets_arena_bytes(sets, nsets, params, results, debug)), "device arena");
     auto take = [&](size_t b) { return w.arena.take(b); };
@@ -398,14 +460,20 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     PHB_TRY(cudaEventRecord(w.ev[5], s), "event");
 
     PHB_TRY(cudaMemcpyAsync(w.pending_err, d_err, 8 * nsets, cudaMemcpyDeviceToHost, s), "D2H status");
-    for (uint32_t i = 0; i < nsets; i++) {
-        if (results[i].on_device) continue;
-        const SetDesc &d = hdesc[i];
-        if (d.partitions)
-            PHB_TRY(cudaMemcpyAsync(results[i].pilots, d.pilots, 4 * (size_t)B * d.partitions, cudaMemcpyDeviceToHost,
-                                    s), "D2H pilots");
-        PHB_TRY(cudaMemcpyAsync(results[i].partition_offsets, d.part_off, 4 * ((size_t)d.partitions + 1),
-                                cudaMemcpyDeviceToHost, s), "D2H offsets");
+    {
+        size_t next = 0;  // pending_copies are in the order of the arrays below
+        char *stage = static_cast<char *>(w.stage.data());
+        auto to_host = [&](void *dst, const void *src, size_t bytes) {
+            if (next < w.pending_copies.size() && w.pending_copies[next].dst == dst)
+                dst = stage + w.pending_copies[next++].off;
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        };
+        for (uint32_t i = 0; i < nsets; i++) {
+            if (results[i].on_device) continue;
+            const SetDesc &d = hdesc[i];
+            if (d.partitions) PHB_TRY(to_host(results[i].pilots, d.pilots, 4 * (size_t)B * d.partitions), "D2H pilots");
+            PHB_TRY(to_host(results[i].partition_offsets, d.part_off, 4 * ((size_t)d.partitions + 1)), "D2H offsets");
+        }
     }
     if (debug) {
         if (dbg->keys4 && N) PHB_TRY(cudaMemcpyAsync(dbg->keys4, d_dbg_keys, 16 * N, cudaMemcpyDeviceToHost, s), "D2H keys");
@@ -444,6 +512,11 @@ phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t,
         st = wait_event(w.ev[6], w.timeout_ms, err);
     }
     if (st != PHOBIC_OK) return st;
+    if (!w.pending_copies.empty()) {
+        StageRange r("copy results to pageable memory");
+        copy_out(w.pending_copies, static_cast<const char *>(w.stage.data()));
+        w.pending_copies.clear();
+    }
     if (t) {
         t->input_transfer = elapsed(w.ev[0], w.ev[1]);
         t->bucket_sizes = elapsed(w.ev[1], w.ev[2]);

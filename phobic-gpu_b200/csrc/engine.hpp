@@ -59,6 +59,14 @@ struct Worker {
     cudaEvent_t ev[8] = {};
     DeviceArena arena;
     PinnedBuffer pinned;  // set table on the way in, per-set error words on the way out
+    // Results bound for pageable host memory are copied into `stage` on the stream and
+    // from there to their destination by finish_sets.
+    struct HostCopy {
+        void *dst;
+        size_t off, bytes;
+    };
+    PinnedBuffer stage;
+    std::vector<HostCopy> pending_copies;
     uint32_t pending_sets = 0;
     uint32_t pending_kernels = 0;  // kernels the last enqueued build launched
     unsigned long long *pending_err = nullptr;  // host view of the error words of the last build

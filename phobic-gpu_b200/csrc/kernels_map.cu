@@ -284,8 +284,7 @@ MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count) {
 template <int KIND, bool SCATTER, bool NARROW>
 static cudaError_t launch_chunk(const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
     const size_t smem = chunk_smem(a.M, NARROW);
-    cudaError_t e = cudaFuncSetAttribute(k_chunk<KIND, SCATTER, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_chunk<KIND, SCATTER, NARROW>, smem);
     if (e != cudaSuccess) return e;
     k_chunk<KIND, SCATTER, NARROW><<<plan.grid, kChunkThreads, smem, st>>>(a);
     return cudaSuccess;

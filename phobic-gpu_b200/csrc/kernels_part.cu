@@ -234,7 +234,7 @@ uint32_t part_wshift(uint64_t partitions) {
 template <int KIND>
 static cudaError_t launch_bin_kind(const MapArgs &a, const PartArgs &p, int grid, cudaStream_t st) {
     const size_t smem = part_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_bin<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_bin<KIND>, smem);
     if (e != cudaSuccess) return e;
     k_bin<KIND><<<grid, kPartThreads, smem, st>>>(a, p);
     return cudaGetLastError();
@@ -254,7 +254,7 @@ cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int 
     }
     if (e != cudaSuccess) return e;
     const size_t smem = part_smem_bytes();
-    e = cudaFuncSetAttribute(k_place, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_dynamic_smem(k_place, smem);
     if (e != cudaSuccess) return e;
     k_place<<<grid, kPartThreads, smem, st>>>(p, a.total_keys, a.lowers, a.bkt);
     return cudaGetLastError();

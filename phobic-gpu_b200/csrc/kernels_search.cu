@@ -625,7 +625,7 @@ cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st) {
     const int warps = search_warps_per_cta(a.buckets, a.cap);
     if (warps < 1) return cudaErrorInvalidValue;
     const size_t smem = (size_t)warps * search_warp_smem(a.buckets, a.cap);
-    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = allow_dynamic_smem(k_search, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search, warps * 32, smem);

@@ -7,8 +7,9 @@
 // dispatcher hands them to stream workers:
 //   * a free worker takes the oldest pending request plus every later pending
 //     request with the same key kind, placement and parameters, up to a batch
-//     limit, and builds them together (one launch per stage, a shared partition
-//     queue in the search kernel);
+//     limit (sets, keys, and the batch's arena size: the reserved arena once
+//     phobic_server_reserve sized the streams), and builds them together (one
+//     launch per stage, a shared partition queue in the search kernel);
 //   * a batch is admitted only while the device memory held by all workers'
 //     arenas stays within the budget; idle workers give their arenas back when
 //     memory is short;
@@ -71,6 +72,7 @@ struct phobic_server {
     // stats
     std::vector<double> latencies;
     uint64_t completed = 0, failed = 0, keys = 0, peak_bytes = 0;
+    uint64_t reserve_bytes = 0;  // arena size set by phobic_server_reserve (0: none)
     double busy_ms = 0;
     int running = 0;
     Clock::time_point busy_since;
@@ -159,19 +161,39 @@ void dispatch_loop(phobic_server *s) {
             }
         if (!free_w) continue;
 
-        // Oldest request first, then later compatible ones (continuous batching).
+        // Oldest request first, then later compatible ones (continuous batching), while the
+        // batch's own arena size stays within the limit: the reserved arena when the server
+        // was sized by phobic_server_reserve (so batches do not grow it), else a worker's
+        // share of the budget.  The head request is always taken.
         std::vector<Request> batch;
+        std::vector<phobic_keys> bkeys;
+        std::vector<phobic_result> bres;
         uint64_t bytes = 0, nkeys = 0;
         const Request head = s->pending.front();
+        const uint64_t limit = s->reserve_bytes ? std::max(s->reserve_bytes, head.bytes)
+                                                : s->cfg.budget_bytes / (uint64_t)s->workers.size() + head.bytes;
         for (auto it = s->pending.begin(); it != s->pending.end();) {
-            if (!batch.empty() && (!same_group(*it, head) || nkeys + it->keys.n > kBatchKeyLimit ||
-                                   (s->cfg.max_batch_sets && batch.size() >= s->cfg.max_batch_sets) ||
-                                   bytes + it->bytes > s->cfg.budget_bytes / (uint64_t)s->workers.size() + head.bytes)) {
-                ++it;
-                continue;
+            uint64_t with = it->bytes;
+            if (!batch.empty()) {
+                bool fits = same_group(*it, head) && nkeys + it->keys.n <= kBatchKeyLimit &&
+                            !(s->cfg.max_batch_sets && batch.size() >= s->cfg.max_batch_sets);
+                if (fits) {
+                    bkeys.push_back(it->keys);
+                    bres.push_back(it->result);
+                    with = sets_arena_bytes(bkeys.data(), (uint32_t)bkeys.size(), &head.params, bres.data(), false);
+                    bkeys.pop_back();
+                    bres.pop_back();
+                    fits = with <= limit;
+                }
+                if (!fits) {
+                    ++it;
+                    continue;
+                }
             }
+            bkeys.push_back(it->keys);
+            bres.push_back(it->result);
             batch.push_back(*it);
-            bytes += it->bytes;
+            bytes = with;
             nkeys += it->keys.n;
             it = s->pending.erase(it);
         }
@@ -312,6 +334,26 @@ phobic_status phobic_server_drain(phobic_server *s, uint32_t timeout_ms) {
     std::unique_lock<std::mutex> lk(s->mu);
     bool ok = s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return s->outstanding == 0; });
     return ok ? PHOBIC_OK : PHOBIC_ERR_TIMEOUT;
+}
+
+phobic_status phobic_server_reserve(phobic_server *s, uint64_t device_bytes, uint64_t pinned_bytes) {
+    if (!s) return PHOBIC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return PHOBIC_ERR_INVALID;
+    if (device_bytes > s->cfg.budget_bytes / s->workers.size()) return PHOBIC_ERR_BUDGET;
+    if (s->outstanding) return PHOBIC_ERR_BUSY;
+    // Idle workers only (nothing outstanding): their threads wait on cv_work and touch
+    // neither the arena nor the stage until the dispatcher hands them a batch.
+    for (auto *sw : s->workers) {
+        std::string err;
+        phobic_status st = cuda_status(cudaSetDevice(sw->w.device), "cudaSetDevice", &err);
+        if (st == PHOBIC_OK && device_bytes) st = cuda_status(sw->w.arena.reserve(device_bytes), "device arena", &err);
+        if (st == PHOBIC_OK && pinned_bytes) st = cuda_status(sw->w.stage.reserve(pinned_bytes), "pinned stage", &err);
+        sw->reserved = sw->w.arena.capacity();
+        if (st != PHOBIC_OK) return st;
+    }
+    s->reserve_bytes = std::max(s->reserve_bytes, device_bytes);
+    return PHOBIC_OK;
 }
 
 phobic_status phobic_server_stats_get(phobic_server *s, phobic_server_stats *out) {

@@ -150,6 +150,7 @@ def _lib() -> C.CDLL:
         "phobic_server_poll": (I32, [P, U64, C.POINTER(I32), C.POINTER(I32)]),
         "phobic_server_wait": (I32, [P, U64, U32, C.POINTER(I32)]),
         "phobic_server_drain": (I32, [P, U32]),
+        "phobic_server_reserve": (I32, [P, U64, U64]),
         "phobic_server_stats_get": (I32, [P, C.POINTER(ServerStats)]),
         "phobic_server_destroy": (I32, [P]),
     }
@@ -539,6 +540,20 @@ class Server:
 
     def drain(self, timeout_ms: int = 600_000) -> None:
         check(_lib().phobic_server_drain(self.handle, timeout_ms))
+
+    def reserve(self, device_bytes: int, pinned_bytes: int = 0) -> None:
+        """Size every stream's device arena and pinned result stage now (phobic_server_reserve)."""
+        check(_lib().phobic_server_reserve(self.handle, device_bytes, pinned_bytes))
+
+    @staticmethod
+    def bytes_for(keys, cfg: MPHFconfig, kind: int | None = None) -> tuple[int, int]:
+        """(device_bytes, pinned_bytes) one request for these keys needs: the arena of
+        phobic_build_bytes_needed and the stage for results bound for pageable memory."""
+        ks = keyset(keys, kind)
+        k = ks.struct()
+        dev = int(_lib().phobic_build_bytes_needed(C.byref(k), C.byref(cfg.params)))
+        parts = cfg.partitions(ks.n)
+        return dev, 4 * (cfg.bucketCountPerPartition * parts + parts + 1) + 512
 
     def stats(self) -> dict:
         s = ServerStats()

@@ -103,3 +103,60 @@ def test_server_budget_admission(phobic):
             st, _ = srv.wait(t)
             assert st == 0
         assert srv.stats()["peak_bytes"] <= need + (1 << 20)
+
+
+def test_server_reserve_sizes_every_stream(phobic):
+    """phobic_server_reserve sizes each stream's arena up front; requests up to that size
+    then build without growing it, and the results equal the plain builds."""
+    cfg = phobic.MPHFconfig(7.0, 2048)
+    big = keygen.splitmix64(12, 3_000_000)
+    dev, pinned = phobic.Server.bytes_for(big, cfg)
+    with phobic.Server(0, streams=3, budget_bytes=3 * dev + (1 << 20)) as srv:
+        with pytest.raises(phobic.PhobicError) as e:
+            srv.reserve(dev + (1 << 21), pinned)
+        assert e.value.status == phobic.ERR_BUDGET
+        srv.reserve(dev, pinned)
+        assert srv.stats()["peak_bytes"] == 0
+        reqs = [big, keygen.splitmix64(13, 1_000_000), keygen.splitmix64(14, 20_000)]
+        tickets = [srv.submit(k, cfg) for k in reqs]
+        outs = [srv.wait(t) for t in tickets]
+        srv.reserve(dev, pinned)  # idle again: a no-op
+        assert srv.stats()["peak_bytes"] <= 3 * dev
+    with phobic.Context(0) as alone:
+        for k, (st, got) in zip(reqs, outs):
+            assert st == 0
+            ref = alone.build(k, cfg)
+            assert (got.pilots == ref.pilots).all() and (got.partition_offsets == ref.partition_offsets).all()
+
+
+def test_concurrent_contexts_with_different_launch_shapes(phobic):
+    """Two contexts build from two host threads at once, with different partition counts
+    and (lambda, P), so their kernels ask for different amounts of shared memory; every
+    build succeeds and equals the same build made alone."""
+    import threading
+
+    jobs = [(phobic.MPHFconfig(7.0, 2500), [20_000, 3_000_000, 200_000, 6_000_000]),
+            (phobic.MPHFconfig(3.0, 1024), [1_000_000, 50_000, 4_000_000])]
+    keys = {n: keygen.splitmix64(900 + n % 97, n) for _, sizes in jobs for n in sizes}
+    errors, firsts = [], {}
+
+    def run(j, cfg, sizes):
+        try:
+            with phobic.Context(0) as c:
+                for r in range(40):
+                    n = sizes[r % len(sizes)]
+                    got = c.build(keys[n], cfg)
+                    firsts.setdefault((j, n), got)
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append(repr(e))
+
+    threads = [threading.Thread(target=run, args=(j, cfg, sizes)) for j, (cfg, sizes) in enumerate(jobs)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    with phobic.Context(0) as alone:
+        for (j, n), got in firsts.items():
+            ref = alone.build(keys[n], jobs[j][0])
+            assert (got.pilots == ref.pilots).all() and (got.partition_offsets == ref.partition_offsets).all()

@@ -127,6 +127,25 @@ def test_device_resident_keys_and_result(phobic, ctx):
     assert ctx.verify(dk, cfg, got) == 0
 
 
+def test_pinned_and_pageable_host_results_agree(phobic, ctx):
+    """Host results go straight to pinned memory and through the worker's pinned stage to
+    pageable memory (5.7 MB of pilots: the copy-out is split over host threads)."""
+    torch = pytest.importorskip("torch")
+    keys = keygen.splitmix64(8, 10_000_000)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    parts, B = cfg.partitions(len(keys)), cfg.bucketCountPerPartition
+    assert 4 * B * parts > 4 << 20
+    pageable = ctx.build(keys, cfg)
+    pil = torch.zeros(B * parts, dtype=torch.int32).pin_memory()
+    off = torch.zeros(parts + 1, dtype=torch.int32).pin_memory()
+    ctx.build(keys, cfg, out=(pil, off))
+    assert (pil.numpy().view(np.uint32) == pageable.pilots).all()
+    assert (off.numpy().view(np.uint32) == pageable.partition_offsets).all()
+    small = keygen.splitmix64(9, 3000)
+    a, b = ctx.build(small, cfg), ctx.build(small, cfg)
+    assert (a.pilots == b.pilots).all() and (a.partition_offsets == b.partition_offsets).all()
+
+
 def test_bijection_at_ten_million(phobic, ctx):
     keys = keygen.splitmix64(5, 10_000_000)
     cfg = phobic.MPHFconfig(7.0, 2500)
