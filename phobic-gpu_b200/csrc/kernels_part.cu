@@ -105,6 +105,10 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
         for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
     const uint64_t tiles = (a.total_keys + kPartTile - 1) / kPartTile;
     SetCache sc;
+    // u64 keys of one set (the plain build): partition ids need no set lookup.
+    const bool raw_u64 = KIND == PHOBIC_KEYS_U64 && a.nsets == 1;
+    const unsigned long long *keys64 = static_cast<const unsigned long long *>(a.sets[0].data);
+    const uint32_t parts0 = a.sets[0].partitions;
     for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         const uint64_t t0 = t * kPartTile;
         const uint32_t count = (uint32_t)(a.total_keys - t0 < (uint64_t)kPartTile ? a.total_keys - t0 : kPartTile);
@@ -112,6 +116,24 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
         __syncthreads();
         uint4 rec[kPartItems];
         uint32_t rank[kPartItems];
+        if (raw_u64) {
+            // All of the tile's key loads of this thread are issued before any key is hashed.
+            unsigned long long raw[kPartItems];
+#pragma unroll
+            for (int j = 0; j < kPartItems; j++) {
+                const uint32_t q = j * kPartThreads + threadIdx.x;
+                raw[j] = q < count ? __ldg(keys64 + t0 + q) : 0ull;
+            }
+#pragma unroll
+            for (int j = 0; j < kPartItems; j++) {
+                const uint32_t q = j * kPartThreads + threadIdx.x;
+                rank[j] = 0xFFFFFFFFu;
+                if (q >= count) continue;
+                const Key4 k = key_from_hash(xxh3::hash_u64(raw[j]));
+                rec[j] = make_uint4(k.lower1, k.lower2, partition_of(k.partitioner, parts0), bucket_of(k.bucketer, sf));
+                if (PHB_CHECK((rec[j].z >> p.wshift) < p.nbins)) rank[j] = atomicAdd(&hist[rec[j].z >> p.wshift], 1u);
+            }
+        } else {
 #pragma unroll
         for (int j = 0; j < kPartItems; j++) {
             const uint32_t q = j * kPartThreads + threadIdx.x;
@@ -128,6 +150,7 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
                                     bucket_of(k.bucketer, sf));
             }
             if (PHB_CHECK((rec[j].z >> p.wshift) < p.nbins)) rank[j] = atomicAdd(&hist[rec[j].z >> p.wshift], 1u);
+        }
         }
         __syncthreads();
         block_exclusive_scan(hist, loff, p.nbins, warp_sums);
