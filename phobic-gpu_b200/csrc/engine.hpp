@@ -67,6 +67,9 @@ struct Worker {
     };
     PinnedBuffer stage;
     std::vector<HostCopy> pending_copies;
+    // Inputs in pageable host memory go up through two pinned chunk buffers (upload()).
+    PinnedBuffer up_stage;
+    cudaEvent_t up_ev[2] = {};
     uint32_t pending_sets = 0;
     uint32_t pending_kernels = 0;  // kernels the last enqueued build launched
     unsigned long long *pending_err = nullptr;  // host view of the error words of the last build

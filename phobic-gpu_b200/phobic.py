@@ -250,6 +250,8 @@ def keyset(keys, kind: int | None = None) -> KeySet:
             return KeySet(KEYS_U64 if kind is None else kind, int(keys.shape[0]), keys.contiguous(), None, True)
         return KeySet(KEYS_BYTES16 if kind is None else kind, int(keys.shape[0]), keys.contiguous(), None, True)
     a = np.ascontiguousarray(keys)
+    if a.dtype == np.int64:  # the same 8 bytes per key: a view, not a copy (a pinned buffer stays pinned)
+        a = a.view(np.uint64)
     if a.ndim == 1:
         return KeySet(KEYS_U64 if kind is None else kind, a.shape[0], a.astype(np.uint64, copy=False))
     if a.ndim == 2 and a.dtype == np.uint64 and a.shape[1] == 2:

@@ -351,3 +351,25 @@ def test_packed_counter_carry_into_the_next_set(phobic, ctx):
     assert st == [w0["status"], w1["status"]]
     if w1["status"] == 0:
         assert (res[1].pilots == w1["pilots"]).all() and (res[1].partition_offsets == w1["offsets"]).all()
+
+
+def test_pageable_host_keys_upload_in_chunks(phobic, ctx):
+    """Host keys in pageable memory go up through the worker's pinned chunk buffers (80 MB of
+    u64 keys: three chunks, both buffers; 11 MB of string bytes); the builds equal the builds
+    from device-resident keys and from pinned keys."""
+    torch = pytest.importorskip("torch")
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(15, 10_000_000)
+    want = ctx.build(torch.from_numpy(keys.view(np.int64)).cuda(), cfg)
+    for host in (keys, torch.from_numpy(keys.view(np.int64)).pin_memory()):
+        got = ctx.build(host, cfg)
+        assert (got.pilots == want.pilots).all() and (got.partition_offsets == want.partition_offsets).all()
+    strs = [b"k%07d-" % i + bytes(keygen.splitmix64(i, 1).view(np.uint8)[: i % 29]) for i in range(300_000)]
+    offs = np.zeros(len(strs) + 1, np.uint64)
+    np.cumsum([len(x) for x in strs], out=offs[1:])
+    data = np.frombuffer(b"".join(strs), np.uint8).copy()
+    assert len(data) > 4 << 20
+    sw = ctx.build((torch.from_numpy(data).cuda(), torch.from_numpy(offs.view(np.int64)).cuda()), cfg)
+    sg = ctx.build((data, offs), cfg)
+    assert (sg.pilots == sw.pilots).all() and (sg.partition_offsets == sw.partition_offsets).all()
+    assert ctx.verify((data, offs), cfg, sg) == 0
