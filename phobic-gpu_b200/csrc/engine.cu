@@ -166,6 +166,50 @@ static phobic_status upload(Worker &w, void *dst, const void *src, size_t bytes,
     return PHOBIC_OK;
 }
 
+// Device-to-host copy of `bytes` into host memory `dst`, complete when this returns (the
+// stream's earlier work included).  Pageable destinations are served in kUpChunk pieces
+// through the two pinned buffers: the copy engine fills one while host threads empty the
+// other.
+static phobic_status download(Worker &w, void *dst, const void *src, size_t bytes, cudaStream_t s, std::string *err) {
+    const bool staged = bytes >= kUpDirect && is_pageable(dst) && w.up_stage.reserve(2 * kUpChunk) == cudaSuccess;
+    cudaGetLastError();
+    if (!staged) {
+        PHB_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s), "D2H");
+        PHB_TRY(cudaEventRecord(w.up_ev[0], s), "event");
+        return wait_event(w.up_ev[0], w.timeout_ms, err);
+    }
+    const int threads = std::max(1, std::min(8, omp_get_max_threads()));
+    char *stage = static_cast<char *>(w.up_stage.data());
+    const size_t chunks = (bytes + kUpChunk - 1) / kUpChunk;
+    auto issue = [&](size_t i) -> phobic_status {
+        const size_t off = i * kUpChunk, len = std::min(kUpChunk, bytes - off);
+        const int b = (int)(i & 1);
+        phobic_status st = wait_event(w.up_ev[b], w.timeout_ms, err);  // an earlier upload's copy is done
+        if (st != PHOBIC_OK) return st;
+        PHB_TRY(cudaMemcpyAsync(stage + b * kUpChunk, static_cast<const char *>(src) + off, len,
+                                cudaMemcpyDeviceToHost, s), "D2H");
+        PHB_TRY(cudaEventRecord(w.up_ev[b], s), "event");
+        return PHOBIC_OK;
+    };
+    phobic_status st = issue(0);
+    if (st == PHOBIC_OK && chunks > 1) st = issue(1);
+    for (size_t i = 0; st == PHOBIC_OK && i < chunks; i++) {
+        const int b = (int)(i & 1);
+        if ((st = wait_event(w.up_ev[b], w.timeout_ms, err)) != PHOBIC_OK) break;
+        const size_t off = i * kUpChunk, len = std::min(kUpChunk, bytes - off);
+        const char *buf = stage + b * kUpChunk;
+        char *to = static_cast<char *>(dst) + off;
+        const int64_t pieces = (int64_t)((len + (1u << 20) - 1) >> 20);
+#pragma omp parallel for num_threads(threads) schedule(static)
+        for (int64_t q = 0; q < pieces; q++) {
+            const size_t lo = (size_t)q << 20, hi = std::min(len, lo + (1u << 20));
+            std::memcpy(to + lo, buf + lo, hi - lo);
+        }
+        if (i + 2 < chunks) st = issue(i + 2);
+    }
+    return st;
+}
+
 phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
     if (e == cudaSuccess) return PHOBIC_OK;
     if (err) *err = std::string(what) + ": " + cudaGetErrorString(e);
@@ -662,11 +706,10 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
     if (!built->on_device) {
         uint32_t *a = static_cast<uint32_t *>(w.arena.take(4 * (size_t)B * partitions));
         uint32_t *b = static_cast<uint32_t *>(w.arena.take(4 * ((size_t)partitions + 1)));
-        if (partitions)
-            PHB_TRY(cudaMemcpyAsync(a, built->pilots, 4 * (size_t)B * partitions, cudaMemcpyHostToDevice, s),
-                    "H2D pilots");
-        PHB_TRY(cudaMemcpyAsync(b, built->partition_offsets, 4 * ((size_t)partitions + 1), cudaMemcpyHostToDevice, s),
-                "H2D offsets");
+        if (partitions && (st = upload(w, a, built->pilots, 4 * (size_t)B * partitions, s, err)) != PHOBIC_OK)
+            return st;
+        if ((st = upload(w, b, built->partition_offsets, 4 * ((size_t)partitions + 1), s, err)) != PHOBIC_OK)
+            return st;
         d_pil = a, d_off = b;
     }
     PHB_TRY(cudaMemcpyAsync(hword, d_off + partitions, 4, cudaMemcpyDeviceToHost, s), "D2H n");
@@ -684,8 +727,9 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
     const int grid = (int)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)w.sm_count * 8);
     if (n && partitions) PHB_TRY(launch_query(keys->kind, data, offs, n, qa, grid, s), "query");
     if (bad) PHB_TRY(cudaMemcpyAsync(hword, d_bad, 8, cudaMemcpyDeviceToHost, s), "D2H");
-    if (positions && !keys->on_device && n)
-        PHB_TRY(cudaMemcpyAsync(positions, d_pos, 4 * n, cudaMemcpyDeviceToHost, s), "D2H positions");
+    if (positions && !keys->on_device && n) {
+        if ((st = download(w, positions, d_pos, 4 * n, s, err)) != PHOBIC_OK) return st;
+    }
     PHB_TRY(cudaEventRecord(w.ev[7], s), "event");
     if ((st = wait_event(w.ev[7], w.timeout_ms, err)) != PHOBIC_OK) return st;
     if (bad) *bad = *hword + (n > n_built ? n - n_built : n_built - n);

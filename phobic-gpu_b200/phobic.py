@@ -337,13 +337,21 @@ class Context:
         return (BuildResult(pil, off, parts, cfg.bucketCountPerPartition), keys4[: ks.n],
                 sizes[: parts * cfg.bucketCountPerPartition].reshape(parts, cfg.bucketCountPerPartition))
 
-    def query(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None) -> np.ndarray:
+    def query(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None):
+        """Slot of every key: a numpy uint32 array for host keys, an int32 CUDA tensor on the
+        keys' device for device-resident keys (phobic_query writes positions where the keys are)."""
         ks = keyset(keys, kind)
-        pos = np.zeros(max(ks.n, 1), np.uint32)
+        if ks.on_device:
+            import torch
+            pos = torch.empty(max(ks.n, 1), dtype=torch.int32, device=ks.data.device)
+            ptr = pos.data_ptr()
+        else:
+            pos = np.zeros(max(ks.n, 1), np.uint32)
+            ptr = pos.ctypes.data
         res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
         k = ks.struct()
         check(_lib().phobic_query(self.handle, C.byref(k), C.byref(cfg.params), built.partitions, C.byref(res),
-                                  pos.ctypes.data), self)
+                                  ptr), self)
         return pos[: ks.n]
 
     def set_memory_limit(self, nbytes: int) -> None:

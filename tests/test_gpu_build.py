@@ -373,3 +373,18 @@ def test_pageable_host_keys_upload_in_chunks(phobic, ctx):
     sg = ctx.build((data, offs), cfg)
     assert (sg.pilots == sw.pilots).all() and (sg.partition_offsets == sw.partition_offsets).all()
     assert ctx.verify((data, offs), cfg, sg) == 0
+
+
+def test_query_host_and_device_positions_agree(phobic, ctx):
+    """Positions of 10M host keys come back through the pinned chunk buffers (40 MB into a
+    numpy array: two chunks); device-resident keys get device positions; both agree and
+    form a bijection onto [0, n)."""
+    torch = pytest.importorskip("torch")
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(16, 10_000_000)
+    built = ctx.build(keys, cfg)
+    host = ctx.query(keys, cfg, built)
+    dev = ctx.query(torch.from_numpy(keys.view(np.int64)).cuda(), cfg, built)
+    assert isinstance(host, np.ndarray) and dev.is_cuda
+    assert (dev.cpu().numpy().view(np.uint32) == host).all()
+    assert O.is_bijection(host)
