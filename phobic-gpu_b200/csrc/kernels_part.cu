@@ -90,6 +90,8 @@ __device__ __forceinline__ void block_exclusive_scan(const uint32_t *cnt, uint32
 
 }  // namespace
 
+static_assert(kMaxBins == (uint32_t)kPartThreads, "k_bin gives every thread at most one bin cursor");
+
 size_t part_smem_bytes() { return sizeof(uint4) * kPartTile; }
 
 // Pass 1.  Shared memory: fulcrums (static), bin counters and bases (static),
@@ -154,12 +156,16 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
         }
         __syncthreads();
         block_exclusive_scan(hist, loff, p.nbins, warp_sums);
-        for (uint32_t b = threadIdx.x; b < p.nbins; b += blockDim.x)
-            if (hist[b]) gbase[b] = atomicAdd(&p.bincur[b], hist[b]) - loff[b];
+        // Thread b takes bin b's cursor (kMaxBins == kPartThreads); the atomic's result is
+        // used only after this thread's stage writes, which run while it is in flight.
+        const uint32_t my_bin = threadIdx.x;
+        const bool has_bin = my_bin < p.nbins && hist[my_bin] != 0;
+        const uint32_t my_cur = has_bin ? atomicAdd(&p.bincur[my_bin], hist[my_bin]) : 0u;
 #pragma unroll
         for (int j = 0; j < kPartItems; j++)
             if (rank[j] != 0xFFFFFFFFu && PHB_CHECK(loff[rec[j].z >> p.wshift] + rank[j] < (uint32_t)kPartTile))
                 stage[loff[rec[j].z >> p.wshift] + rank[j]] = rec[j];
+        if (has_bin) gbase[my_bin] = my_cur - loff[my_bin];
         __syncthreads();
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
@@ -222,18 +228,24 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
             rank[j] = q < count ? atomicAdd(&hist[rec[j].z - gmin], 1u) : 0xFFFFFFFFu;
         }
         __syncthreads();
-        block_exclusive_scan(hist, base, range, warp_sums);  // base = local offsets for now
+        block_exclusive_scan(hist, base, range, warp_sums);  // base = local offsets
+        // Partition cursors: thread i's first partition's atomic is issued before its stage
+        // writes and used after them; hist[i] becomes the global base of partition
+        // gmin + i less its local offset (hist is free once the scan has read it).
+        const uint32_t i0 = threadIdx.x;
+        const bool has0 = i0 < range && hist[i0] != 0;
+        const uint32_t cur0 = has0 ? atomicAdd(&p.pcur[gmin + i0], hist[i0]) : 0u;
 #pragma unroll
         for (int j = 0; j < kPartItems; j++)
             if (rank[j] != 0xFFFFFFFFu && PHB_CHECK(base[rec[j].z - gmin] + rank[j] < (uint32_t)kPartTile))
                 stage[base[rec[j].z - gmin] + rank[j]] = rec[j];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < range; i += blockDim.x)
-            if (hist[i]) base[i] = atomicAdd(&p.pcur[gmin + i], hist[i]) - base[i];
+        if (has0) hist[i0] = cur0 - base[i0];
+        for (uint32_t i = i0 + blockDim.x; i < range; i += blockDim.x)
+            if (hist[i]) hist[i] = atomicAdd(&p.pcur[gmin + i], hist[i]) - base[i];
         __syncthreads();
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
-            const uint32_t dst = base[r.z - gmin] + q;
+            const uint32_t dst = hist[r.z - gmin] + q;
             if (!PHB_CHECK(dst < total)) continue;
             lowers[dst] = make_uint2(r.x, r.y);
             bkt[dst] = (uint16_t)r.w;
