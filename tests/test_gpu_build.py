@@ -294,6 +294,19 @@ def test_packed_counter_builds_match_oracle(phobic, ctx, kind):
     check_against_oracle(phobic, ctx, keys, k, 5.0, 200)
 
 
+def test_packed_counter_strings_match_oracle(phobic, ctx):
+    """Strings through the packed 16-bit counters: 12M strings of 11..24 bytes, 60 000
+    partitions; pilots and offsets equal the oracle's (the string kernels hash ragged
+    rows, a separate instance of K1's counting kernel)."""
+    cfg = phobic.MPHFconfig(5.0, 200)
+    d, o = keygen.strings(46, 12_000_000, 11, 24)
+    assert 52 * 1024 < cfg.partitions(len(o) - 1) <= 104 * 1024
+    want = oracle_build(O.hash_keys((d, o), "strings"), cfg)
+    assert want["status"] == 0
+    got = ctx.build((d, o), cfg)
+    assert (got.pilots == want["pilots"]).all() and (got.partition_offsets == want["offsets"]).all()
+
+
 def test_packed_counter_batch_matches_oracle(phobic, ctx):
     """Eight sets whose 58 000 partitions together take the packed plan."""
     cfg = phobic.MPHFconfig(6.0, 200)
