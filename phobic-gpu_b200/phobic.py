@@ -321,6 +321,7 @@ class Context:
     def build(self, keys, cfg: MPHFconfig, out=None, kind: int | None = None) -> BuildResult:
         ks = keyset(keys, kind)
         res, pil, off, parts = self._result(cfg, ks.n, out)
+        _torch_first(self, ks.data, ks.offsets, pil, off)
         t = Timings()
         k = ks.struct()
         check(_lib().phobic_build(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(t)), self)
@@ -331,6 +332,7 @@ class Context:
         res, pil, off, parts = self._result(cfg, ks.n)
         keys4 = np.zeros((max(ks.n, 1), 4), np.uint32)
         sizes = np.zeros(max(parts * cfg.bucketCountPerPartition, 1), np.uint32)
+        _torch_first(self, ks.data, ks.offsets)
         k = ks.struct()
         check(_lib().phobic_debug_build(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res),
                                         keys4.ctypes.data, sizes.ctypes.data), self)
@@ -349,6 +351,7 @@ class Context:
             pos = np.zeros(max(ks.n, 1), np.uint32)
             ptr = pos.ctypes.data
         res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
+        _torch_first(self, ks.data, ks.offsets, built.pilots, built.partition_offsets, pos)
         k = ks.struct()
         check(_lib().phobic_query(self.handle, C.byref(k), C.byref(cfg.params), built.partitions, C.byref(res),
                                   ptr), self)
@@ -377,6 +380,7 @@ class Context:
         ks = keyset(keys, kind)
         res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
         bad = C.c_uint64()
+        _torch_first(self, ks.data, ks.offsets, built.pilots, built.partition_offsets)
         k = ks.struct()
         check(_lib().phobic_verify(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(bad)), self)
         return int(bad.value)
@@ -384,6 +388,16 @@ class Context:
 
 def _is_cuda(x) -> bool:
     return bool(getattr(x, "is_cuda", False))
+
+
+def _torch_first(ctx: "Context", *bufs) -> None:
+    """Work queued on torch's current stream may still be writing these device tensors
+    (keys made on the GPU, outputs just zeroed).  The context's stream waits for it, by
+    an event (no host synchronisation).  The library's calls return once their work is
+    done, so later torch work sees complete results."""
+    if any(_is_cuda(b) for b in bufs):
+        import torch
+        torch.cuda.ExternalStream(ctx.stream_handle()).wait_stream(torch.cuda.current_stream())
 
 
 class MPHFbuilder:
@@ -432,6 +446,7 @@ def encode_gpu(ctx: "Context", built: BuildResult, cfg: MPHFconfig, pilot_encode
     place) or numpy arrays.  With out (a torch CUDA uint8 tensor) the bytes are
     written there and None is returned in their place."""
     res = Result(int(_is_cuda(built.pilots)), _ptr(built.pilots), _ptr(built.partition_offsets))
+    _torch_first(ctx, built.pilots, built.partition_offsets, out)
     size, bpk = C.c_size_t(), C.c_double()
     args = (ctx.handle, PILOT_ENCODERS[pilot_encoder], OFFSET_ENCODERS[offset_encoder], C.byref(res),
             built.partitions, C.byref(cfg.params))
@@ -500,6 +515,7 @@ def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None 
         outs.append(BuildResult(pil, off, parts, cfg.bucketCountPerPartition))
         res_structs.append(r)
     rarr = (Result * len(kss))(*res_structs)
+    _torch_first(ctx, *[b for ks in kss for b in (ks.data, ks.offsets)], *[b for o in outs for b in (o.pilots, o.partition_offsets)])
     st = (C.c_int * len(kss))()
     t = Timings()
     rc = _lib().phobic_build_batch(ctx.handle, arr, len(kss), C.byref(cfg.params), rarr, st, C.byref(t))
@@ -531,6 +547,11 @@ class Server:
         else:
             pil, off = out
         res = Result(int(_is_cuda(pil)), _ptr(pil), _ptr(off))
+        if any(_is_cuda(b) for b in (ks.data, ks.offsets, pil, off)):
+            # The worker stream that will run the build is chosen later: let torch's
+            # queued writes to these tensors finish first.
+            import torch
+            torch.cuda.current_stream().synchronize()
         k = ks.struct()
         t = C.c_uint64()
         check(_lib().phobic_server_submit(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(t)))

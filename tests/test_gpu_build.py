@@ -401,3 +401,31 @@ def test_query_host_and_device_positions_agree(phobic, ctx):
     assert isinstance(host, np.ndarray) and dev.is_cuda
     assert (dev.cpu().numpy().view(np.uint32) == host).all()
     assert O.is_bijection(host)
+
+
+def test_device_keys_still_being_written_by_torch(phobic, ctx):
+    """Keys that torch is still writing (a copy queued behind 0.1 s of work on torch's
+    current stream) are read only after that work: the build, the query and a server
+    request equal the builds from settled keys."""
+    torch = pytest.importorskip("torch")
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(17, 1_000_000)
+    src = torch.from_numpy(keys.view(np.int64)).cuda()
+    torch.cuda.synchronize()
+    want = ctx.build(keys, cfg)
+    spin = 200_000_000  # clock cycles of torch's spin kernel: about 0.1 s
+
+    def late_keys():
+        dst = torch.zeros_like(src)
+        torch.cuda.synchronize()
+        torch.cuda._sleep(spin)
+        dst.copy_(src)
+        return dst
+
+    got = ctx.build(late_keys(), cfg)
+    assert (got.pilots == want.pilots).all() and (got.partition_offsets == want.partition_offsets).all()
+    pos = ctx.query(late_keys(), cfg, want)
+    assert (pos.cpu().numpy().view(np.uint32) == ctx.query(keys, cfg, want)).all()
+    with phobic.Server(0, streams=2, budget_bytes=4 << 30) as srv:
+        st, r = srv.wait(srv.submit(late_keys(), cfg))
+    assert st == 0 and (r.pilots == want.pilots).all()
