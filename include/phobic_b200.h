@@ -51,7 +51,9 @@ typedef enum phobic_status {
     PHOBIC_ERR_BUDGET = 9,             /* request does not fit the server's memory budget */
     PHOBIC_ERR_BUSY = 10,              /* server queue full */
     PHOBIC_ERR_NO_DEVICE = 11,         /* no CUDA device / not sm_100 */
-    PHOBIC_ERR_NOT_FOUND = 12          /* unknown server ticket */
+    PHOBIC_ERR_NOT_FOUND = 12,         /* unknown server ticket */
+    PHOBIC_ERR_KEYS_CHANGED = 13       /* the build's passes read different keys: device keys were
+                                          written while the build ran (order them before the call) */
 } phobic_status;
 
 /* Key kinds (hasher.hpp:22-66). */

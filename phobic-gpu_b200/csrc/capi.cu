@@ -34,6 +34,7 @@ const char *phobic_status_string(phobic_status s) {
     case PHOBIC_ERR_BUSY: return "queue full";
     case PHOBIC_ERR_NO_DEVICE: return "no suitable CUDA device";
     case PHOBIC_ERR_NOT_FOUND: return "unknown ticket";
+    case PHOBIC_ERR_KEYS_CHANGED: return "keys changed during the build";
     }
     return "unknown status";
 }

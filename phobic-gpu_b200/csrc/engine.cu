@@ -531,7 +531,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         PHB_TRY(launch_scan(sa, s), "K2 scan");
     }
     const uint32_t wshift = part_wshift(M);
-    PartArgs pa{d_inter, d_bincur, d_pcur, wshift, (uint32_t)((M + (1ull << wshift) - 1) >> wshift)};
+    PartArgs pa{d_inter, d_bincur, d_pcur, wshift, (uint32_t)((M + (1ull << wshift) - 1) >> wshift), (uint32_t)M};
     PHB_TRY(launch_check_sizes(d_G, (uint32_t)M, plan.stride, cap, d_pb, nsets, d_err, &pa, s), "K2 size check");
     PHB_TRY(cudaEventRecord(w.ev[3], s), "event");
     {
@@ -540,7 +540,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     }
     PHB_TRY(cudaEventRecord(w.ev[4], s), "event");
     SearchArgs qa{d_desc, d_pb, nsets, (uint32_t)M, d_G, plan.stride, d_lowers, d_bkt, d_sorted, d_dbg_sizes, B, cap,
-                  k_max, d_queue, d_err};
+                  k_max, d_queue, d_err, d_pcur};
     {
         StageRange r("search (K4)");
         PHB_TRY(launch_search(qa, w.sm_count, s), "K4 search");
@@ -589,6 +589,8 @@ static const char *error_text(uint32_t code) {
     case PHOBIC_ERR_SEARCH_LIMIT: return "pilot counter reached its limit";
     case PHOBIC_ERR_TIMEOUT: return "bounded device wait expired";
     case PHOBIC_ERR_DUPLICATE_KEY: return "two keys of one bucket hash identically (duplicate keys)";
+    case PHOBIC_ERR_KEYS_CHANGED:
+        return "the passes of the build read different keys (device keys written while the build ran)";
     default: return "error";
     }
 }

@@ -105,6 +105,7 @@ struct PartArgs {
     uint32_t *pcur;     // [M] cursors, start = partition offset
     uint32_t wshift;    // coarse bin = partition >> wshift
     uint32_t nbins;     // ceil(M / 2^wshift) <= kMaxBins
+    uint32_t M;         // partitions (records naming another are not placed)
 };
 // Smallest shift giving at most kTargetBins coarse bins, lowered (up to kMaxBins bins)
 // until two bins span at most kLocalRange partitions.
@@ -138,6 +139,9 @@ struct SearchArgs {
     uint32_t k_max;
     uint32_t *queue;            // zeroed job counter
     unsigned long long *err;    // [nsets]
+    // [M] placement cursors after K3 (or null): partition g must end at its scanned offset,
+    // else its keys differed between K1 and K3.
+    const uint32_t *placed = nullptr;
 };
 
 struct QueryArgs {

@@ -170,7 +170,9 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_bin(MapArgs a, PartArgs p) 
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
             const uint64_t dst = (uint64_t)gbase[r.z >> p.wshift] + q;
-            if (PHB_CHECK(dst < a.total_keys)) p.inter[dst] = r;
+            // dst >= total only when counts and keys disagree (the keys changed; K4 reports
+            // it): the clamp keeps that store inside the array.
+            if (PHB_CHECK(dst < a.total_keys)) p.inter[min(dst, a.total_keys - 1)] = r;
         }
         __syncthreads();
     }
@@ -206,12 +208,17 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
         }
         __syncthreads();
         const uint32_t gmin = s_min, range = s_max - s_min + 1;
+        if (s_max >= p.M) {  // a record of no partition: pass 1 left it unwritten (the keys changed)
+            (void)PHB_CHECK(false);
+            __syncthreads();
+            continue;
+        }
         if (range > kLocalRange) {  // partitions too small for runs: one atomic per record
 #pragma unroll
             for (int j = 0; j < kPartItems; j++) {
                 const uint32_t q = j * kPartThreads + threadIdx.x;
                 if (q >= count) continue;
-                const uint32_t dst = atomicAdd(&p.pcur[rec[j].z], 1u);
+                const uint32_t dst = (uint32_t)min((uint64_t)atomicAdd(&p.pcur[rec[j].z], 1u), total - 1);
                 if (!PHB_CHECK(dst < total)) continue;
                 lowers[dst] = make_uint2(rec[j].x, rec[j].y);
                 bkt[dst] = (uint16_t)rec[j].w;
@@ -245,7 +252,8 @@ __global__ void __launch_bounds__(kPartThreads, 2) k_place(PartArgs p, uint64_t 
         __syncthreads();
         for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
             const uint4 r = stage[q];
-            const uint32_t dst = hist[r.z - gmin] + q;
+            // Clamped: only a build whose keys changed (reported by K4) gets past total.
+            const uint32_t dst = (uint32_t)min((uint64_t)(hist[r.z - gmin] + q), total - 1);
             if (!PHB_CHECK(dst < total)) continue;
             lowers[dst] = make_uint2(r.x, r.y);
             bkt[dst] = (uint16_t)r.w;

@@ -461,9 +461,14 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
                                                      uint32_t g, uint32_t p, int lane) {
     const uint32_t B = a.buckets;
     const uint32_t base = a.G[(size_t)g * a.gstride];
-    const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
+    const uint32_t end = a.G[(size_t)(g + 1) * a.gstride];
+    // K3 placed exactly the keys K1 counted, unless the keys changed in between (loaded
+    // with the offsets, so the check adds no wait).
+    const uint32_t placed = a.placed ? a.placed[g] : end;
+    const uint32_t ps = end - base;
     if (ps > a.cap) return PHOBIC_OK;  // reported by the size check
     if (!PHB_CHECK(base + ps <= a.G[(size_t)a.M * a.gstride])) return PHOBIC_OK;
+    if (placed != end) return PHOBIC_ERR_KEYS_CHANGED;
     const uint32_t ow = bitmap_words(a.cap);
     uint32_t *pil = d.pilots + p;
     const size_t pstride = d.partitions;

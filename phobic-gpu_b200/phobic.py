@@ -29,7 +29,7 @@ FULCRUMS = 2048
 
 OK, ERR_INVALID, ERR_OOM, ERR_BUCKET_OVERFLOW, ERR_PARTITION_OVERFLOW = 0, 1, 2, 3, 4
 ERR_SEARCH_LIMIT, ERR_TIMEOUT, ERR_CUDA, ERR_DUPLICATE_KEY, ERR_BUDGET = 5, 6, 7, 8, 9
-ERR_BUSY, ERR_NO_DEVICE, ERR_NOT_FOUND = 10, 11, 12
+ERR_BUSY, ERR_NO_DEVICE, ERR_NOT_FOUND, ERR_KEYS_CHANGED = 10, 11, 12, 13
 KEYS_U64, KEYS_BYTES16, KEYS_PREHASHED, KEYS_STRINGS = 0, 1, 2, 3
 BUCKETER_OPT, BUCKETER_UNIFORM, BUCKETER_SKEW = 0, 1, 2
 

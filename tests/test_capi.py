@@ -67,8 +67,9 @@ def test_partitions_formula(phobic):
 
 def test_status_strings(phobic):
     lib = phobic.lib()
-    for s in range(13):
-        assert lib.phobic_status_string(s)
+    for s in range(14):
+        assert lib.phobic_status_string(s) and lib.phobic_status_string(s) != b"unknown status"
+    assert lib.phobic_status_string(phobic.ERR_KEYS_CHANGED) == b"keys changed during the build"
     assert lib.phobic_status_string(999) == b"unknown status"
 
 
