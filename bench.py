@@ -12,9 +12,17 @@ Our arm prints one JSON line with
           events on the library's own launching stream (max over ranks);
   e2e     the same metric through phobic_build with pinned HOST keys and HOST result
           arrays: every step copies the keys in and the pilots/offsets out;
-  roofline  the search kernel (K4, the dominant one) against measured HBM bandwidth;
-  cpu_baseline  the oracle port of the reference's pipeline on this host's cores.
-The reference arm (--impl reference) times that CPU pipeline on the same workload.
+  roofline  the search kernel (K4, the dominant one): algorithmic integer operations
+          (16 per pilot-hash evaluation, 2 per bitmap probe, counted by the oracle on the
+          same keys) per second against the device's measured integer peak, with its
+          issue rate and HBM figures beside it;
+  batched the 4096-set batched build against 4096 plain sequential builds (every set
+          compared with its plain build);
+  served  a slice of the Poisson request stream, served with continuous batching and
+          one request at a time: p50/p99 latency and Mkeys/s;
+  cpu_baseline  the oracle port of the reference's pipeline on this host's cores,
+          building the same 100M keys.
+The reference arm (--impl reference) times that CPU pipeline on the same 100M keys.
 Under torchrun every rank builds its own independent key set (weak scaling, no
 collective on the data path); rank 0 prints.
 """
@@ -110,61 +118,63 @@ def dist_setup():
     return info.world, info.rank, info.local
 
 
-def cpu_baseline(n_sample: int, min_seconds: float = 10.0, max_reps: int = 6) -> dict:
-    """Oracle port of the reference pipeline (host hash + stages + search), all host threads."""
+def oracle_pipeline(keys, cores: int):
+    """One construction by the oracle port (host hash + all stages + search): (s, stats)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import orc  # the oracle: CPU restatement of the reference's construction
 
+    B, f = orc.config(LAMBDA, PSIZE)
+    t0 = time.perf_counter()
+    r = orc.build(orc.hash_keys(keys, "u64", threads=cores), PSIZE, B, f, threads=cores)
+    dt = time.perf_counter() - t0
+    assert r["status"] == 0, r["status"]
+    return dt, r["stats"]
+
+
+def cpu_baseline(n: int, min_seconds: float = 10.0, max_reps: int = 12) -> dict:
+    """Oracle port of the reference pipeline on all host threads, on the same n keys as
+    the GPU arm (seed 2); also returns the search's work counters of that build."""
     import keygen
 
-    keys = keygen.splitmix64(SEED, n_sample)
-    B, f = orc.config(LAMBDA, PSIZE)
+    keys = keygen.splitmix64(SEED, n)
     cores = os.cpu_count() or 1
-    times = []
+    times, stats = [], None
     t_start = time.perf_counter()
     while len(times) < max_reps and (time.perf_counter() - t_start < min_seconds or len(times) < 2):
-        t0 = time.perf_counter()
-        k4 = orc.hash_keys(keys, "u64", threads=cores)
-        r = orc.build(k4, PSIZE, B, f, threads=cores)
-        times.append(time.perf_counter() - t0)
-        assert r["status"] == 0
+        dt, stats = oracle_pipeline(keys, cores)
+        times.append(dt)
     best = min(times)
-    return {"value": n_sample / best / 1e6, "unit": "Mkeys/s", "cores": cores, "kind": "port",
-            "sample": f"first {n_sample} keys of the workload (same lambda/P), {len(times)} runs, best taken",
-            "seconds": sum(times)}
+    return {"value": n / best / 1e6, "unit": "Mkeys/s", "cores": cores, "kind": "port",
+            "sample": f"the whole workload ({n} keys, same seed, lambda, P), {len(times)} runs, best taken",
+            "seconds": sum(times),
+            "_stats": {"hash_evals": int(stats.hash_evals), "probe_keys": int(stats.probe_keys),
+                       "probe_windows": int(stats.probe_words), "k_retries": int(stats.k_retries)}}
 
 
 def run_reference(args) -> None:
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import orc
-
     import keygen
 
-    n = args.ref_sample
+    n = args.n
     keys = keygen.splitmix64(SEED, n)
-    B, f = orc.config(LAMBDA, PSIZE)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
-        orc.build(orc.hash_keys(keys, "u64", threads=cores), PSIZE, B, f, threads=cores)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        r = orc.build(orc.hash_keys(keys, "u64", threads=cores), PSIZE, B, f, threads=cores)
-        times.append(time.perf_counter() - t0)
-        assert r["status"] == 0
+        oracle_pipeline(keys, cores)
+    times = [oracle_pipeline(keys, cores)[0] for _ in range(args.steps)]
     ms = 1e3 * sum(times) / len(times)
     value = n / (ms / 1e3) / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (splitmix64 seed 2)",
-        "config": {"workload": CONFIG_NAME, "n_keys_per_step": n, "lambda": LAMBDA, "partition_size": PSIZE,
-                   "note": "CPU oracle restatement of the reference pipeline (its Vulkan path cannot run here)"},
+        "config": {"workload": workload_name(n), "n_keys": n, "lambda": LAMBDA, "alpha": 1.0,
+                   "partition_size": PSIZE,
+                   "note": "CPU oracle restatement of the reference pipeline (its Vulkan path cannot run here): "
+                           "host XXH128 + every stage + pilot search, each step one whole build of the n keys"},
         "cpu_baseline": {"value": value, "unit": "Mkeys/s", "cores": cores, "kind": "port",
-                         "sample": f"{n} keys per step of the headline workload"},
+                         "sample": f"the whole workload ({n} keys) per step"},
         "e2e": {"value": value, "unit": "Mkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -284,16 +294,15 @@ def run_ours(args) -> None:
         return
     peaks = measured_peaks()
     k4_ms = statistics.mean(search_ms)
-    achieved = K4_BYTES_PER_KEY * n / (k4_ms / 1e3) / 1e9
+    hbm_achieved = K4_BYTES_PER_KEY * n / (k4_ms / 1e3) / 1e9
     traffic = None
     tp = ROOT / "profiles" / "k4_traffic.json"
     if tp.exists():
         tr = json.loads(tp.read_text())
         traffic = tr.get("bytes_per_key", 0) * n if tr.get("bytes_per_key") else None
-    # Issue-rate view of K4 (it is bound by instruction issue, not HBM): warp
-    # instructions per launch from the ncu capture of the same kernel (per partition,
-    # scaled by partitions) over the K4 event time, against 4 schedulers per SM at the
-    # SM clock sampled during the timed region.
+    # Issue-rate view of K4: warp instructions per launch from the ncu capture of the
+    # same kernel (per partition, scaled by partitions) over the K4 event time, against
+    # 4 schedulers per SM at the SM clock sampled during the timed region.
     issue = None
     ip = ROOT / "profiles" / "k4_issue.json"
     clk = clocks.summary()
@@ -306,7 +315,32 @@ def run_ours(args) -> None:
         issue = {"warp_inst_per_launch": inst, "achieved": ach, "peak": peak_issue, "unit": "warp-inst/s",
                  "frac": ach / peak_issue, "sm_count": sms, "sm_mhz": clk["sm_mhz"],
                  "source": "profiles/k4_issue.json (ncu smsp__inst_executed per partition x partitions)"}
-    base = cpu_baseline(args.cpu_sample) if not args.no_cpu_baseline else None
+    base = cpu_baseline(n) if not args.no_cpu_baseline else None
+    # K4's roofline: algorithmic integer operations of the pilot search (the oracle's counts
+    # for these very keys: 16 per pilot-hash evaluation H, 2 per bitmap probe Pr of one key's
+    # 64-offset window) over the K4 event time, against this device's integer peak for the
+    # hash's instruction mix, measured now by the library (phobic_measure_int_peak).
+    counts = base.pop("_stats") if base else None
+    if counts is None:
+        cp = ROOT / "profiles" / "k4_intops.json"
+        counts = json.loads(cp.read_text()) if cp.exists() and n == 100_000_000 else None
+    int_peak, int_peak_ms = ctx.int_peak()
+    roofline = {"kernel": "k_search (K4)", "bound": "issue", "unit": "int-op/s", "peak": int_peak,
+                "peak_source": f"measured: phobic_measure_int_peak, {int_peak_ms:.2f} ms kernel, this run",
+                "launch_ms": k4_ms, "traffic": traffic, "issue": issue,
+                "hbm": {"achieved": hbm_achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                        "frac": hbm_achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                        "bytes_per_key": K4_BYTES_PER_KEY}}
+    if counts:
+        int_ops = 16 * counts["hash_evals"] + 2 * counts["probe_keys"]
+        roofline.update({"achieved": int_ops / (k4_ms / 1e3), "frac": int_ops / (k4_ms / 1e3) / int_peak,
+                         "int_ops_per_launch": int_ops, "hash_evals": counts["hash_evals"],
+                         "probe_keys": counts["probe_keys"], "formula": "16*hash_evals + 2*probe_keys"})
+    extra = {}
+    if world == 1 and not args.no_extra:
+        ctx_b.close()
+        extra["batched"] = c4_leg(args)
+        extra["served"] = c5_leg(args, args.served_seconds)
     line = {
         "metric": METRIC, "value": value, "unit": "Mkeys/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -325,10 +359,8 @@ def run_ours(args) -> None:
                 "single": {"value": world * n / (single_ms / 1e3) / 1e6, "ms_per_step": single_ms,
                            "device_ms_per_step": statistics.mean(e2e_dev),
                            "how": "one build at a time on one context"}},
-        "roofline": {"kernel": "k_search (K4)", "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "peak_source": peaks["source"], "bytes_per_key": K4_BYTES_PER_KEY,
-                     "launch_ms": k4_ms, "issue": issue},
+        "roofline": roofline,
+        **extra,
         "encoding": {"encoder": "interleaved<dictionary> + diff<compact>", "ms": encode_ms,
                      "bits_per_key": bits_per_key, "bytes": len(blob), "host_threads": os.cpu_count(),
                      "e2e_with_encoding_mkeys_s": world * n / ((e2e_ms + encode_ms) / 1e3) / 1e6},
@@ -341,7 +373,8 @@ def run_ours(args) -> None:
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
-    ctx_b.close()
+    if not extra:
+        ctx_b.close()
     ctx.close()
     grp.close()
 
@@ -414,9 +447,10 @@ def run_plain_workload(args, name, lam, P, make_keys, describe) -> None:
     ctx.close()
 
 
-def run_c4(args) -> None:
+def c4_leg(args) -> dict:
     """Batched build: 4096 u64 key sets, sizes log-uniform in [1K, 4M] (seed 4), lambda 6,
-    P 2048, all sets in one batch vs 4096 plain sequential builds on the same GPU."""
+    P 2048, all sets in one batch vs 4096 plain sequential builds on the same GPU.  Every
+    set's batched result is compared with its plain build."""
     import torch
 
     import keygen
@@ -430,30 +464,34 @@ def run_c4(args) -> None:
     keys = keygen.splitmix64_cuda(4, total)  # one stream split into the sets: unique keys
     starts = np.concatenate([[0], np.cumsum(sizes)])
     sets = [keys[int(starts[i]):int(starts[i + 1])] for i in range(len(sizes))]
-    outs = []
-    for n in sizes:
-        parts = cfg.partitions(int(n))
-        outs.append((torch.empty(parts * B, dtype=torch.int32, device="cuda"),
-                     torch.empty(parts + 1, dtype=torch.int32, device="cuda")))
+    parts = [cfg.partitions(int(n)) for n in sizes]
+    pstart = np.concatenate([[0], np.cumsum([B * m for m in parts])])
+    ostart = np.concatenate([[0], np.cumsum([m + 1 for m in parts])])
+    flat = {mode: (torch.empty(int(pstart[-1]), dtype=torch.int32, device="cuda"),
+                   torch.empty(int(ostart[-1]), dtype=torch.int32, device="cuda")) for mode in ("batched", "plain")}
+
+    def outs(mode):
+        fp, fo = flat[mode]
+        return [(fp[int(pstart[i]):int(pstart[i + 1])], fo[int(ostart[i]):int(ostart[i + 1])]) for i in range(len(sets))]
+
     ctx = phobic.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
-    phobic.build_batch(ctx, sets, cfg, outs_in=outs)  # warm-up: grows the arena
+    ob, op = outs("batched"), outs("plain")
+    phobic.build_batch(ctx, sets, cfg, outs_in=ob)  # warm-up: grows the arena
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    res, st = phobic.build_batch(ctx, sets, cfg, outs_in=outs)
+    res, st = phobic.build_batch(ctx, sets, cfg, outs_in=ob)
     batch_wall = time.perf_counter() - t0
     batch_dev = res[0].timings["total"]
-    assert all(x == 0 for x in st)
-    batched_pilots = [o[0].clone() for o in outs[:: max(1, len(outs) // 64)]]
-    # plain sequential builds of the same sets
-    for k in sets[:8]:
-        ctx.build(k, cfg, out=outs[0] if len(k) == len(sets[0]) else None)
+    assert all(x == 0 for x in st), st
+    for k, o in zip(sets[:8], op[:8]):  # warm-up of the plain path
+        ctx.build(k, cfg, out=o)
     lat = []
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     a.record(stream)
-    for k, o in zip(sets, outs):
+    for k, o in zip(sets, op):
         t1 = time.perf_counter()
         ctx.build(k, cfg, out=o)
         lat.append(1e3 * (time.perf_counter() - t1))
@@ -461,24 +499,28 @@ def run_c4(args) -> None:
     torch.cuda.synchronize()
     seq_wall = time.perf_counter() - t0
     seq_dev = a.elapsed_time(b)
-    same = all(bool(torch.equal(p, o[0])) for p, o in zip(batched_pilots, outs[:: max(1, len(outs) // 64)]))
-    bad = sum(ctx.verify(sets[i], cfg, phobic.BuildResult(outs[i][0], outs[i][1], cfg.partitions(len(sets[i])), B))
-              for i in range(0, len(sets), max(1, len(sets) // 32)))
-    print(json.dumps({
-        "workload": "C4 batched build", "sets": len(sizes), "total_keys": total,
-        "config": {"lambda": lam, "partition_size": P, "sizes": "log-uniform [1e3, 4*2^20], seed 4", "data": "synthetic"},
-        "batched": {"wall_ms": 1e3 * batch_wall, "device_ms": batch_dev, "mkeys_per_s": total / batch_wall / 1e6,
-                    "kernel_launches": res[0].timings["kernels"]},
-        "sequential_plain": {"wall_ms": 1e3 * seq_wall, "device_ms": seq_dev, "mkeys_per_s": total / seq_wall / 1e6,
-                             "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                             "kernel_launches": 4 * len(sets)},
-        "speedup_batched_vs_sequential": seq_wall / batch_wall,
-        "batched_equals_plain_sample": same, "bijection_bad_sample": bad,
-    }), flush=True)
+    same = bool(torch.equal(flat["batched"][0], flat["plain"][0])) and bool(torch.equal(flat["batched"][1],
+                                                                                       flat["plain"][1]))
+    bad = sum(ctx.verify(sets[i], cfg, phobic.BuildResult(ob[i][0], ob[i][1], parts[i], B))
+              for i in range(0, len(sets), max(1, len(sets) // 64)))
     ctx.close()
+    del keys, sets, flat, ob, op
+    torch.cuda.empty_cache()
+    return {
+        "workload": "batched build, 4096 u64 key sets log-uniform in [1e3, 4*2^20] (seed 4), lambda 6, P 2048",
+        "sets": len(sizes), "total_keys": total,
+        "mkeys_per_s": total / batch_wall / 1e6, "wall_ms": 1e3 * batch_wall, "device_ms": batch_dev,
+        "kernel_launches": res[0].timings["kernels"],
+        "plain": {"mkeys_per_s": total / seq_wall / 1e6, "wall_ms": 1e3 * seq_wall, "device_ms": seq_dev,
+                  "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                  "kernel_launches": 6 * len(sets), "how": "4096 phobic_build calls in sequence, one context"},
+        "speedup_vs_plain": seq_wall / batch_wall,
+        "all_sets_equal_plain": same, "bijection_bad_sample_of_64": bad,
+        "how": "one phobic_build_batch call (wall clock; device_ms from its events), keys and results on the device",
+    }
 
 
-def run_c5(args) -> None:
+def c5_leg(args, seconds: float) -> dict:
     """Served stream: Poisson arrivals at 200 req/s, sizes log-uniform in [1e4, 5e7], 70 % u64 /
     30 % strings (seed 5), lambda 7, P 2048, device budget 120 GB; continuous batching on
     several streams vs plain one-at-a-time builds (one stream, no batching) of the same stream."""
@@ -489,13 +531,11 @@ def run_c5(args) -> None:
 
     lam, P = 7.0, 2048
     cfg = phobic.MPHFconfig(lam, P)
-    times, sizes, kinds = keygen.request_stream(5, 200.0, args.c5_seconds, 1e4, args.c5_max, 0.3)
+    times, sizes, kinds = keygen.request_stream(5, 200.0, seconds, 1e4, args.c5_max, 0.3)
     rng = np.random.default_rng(55)
     u64_pool = keygen.splitmix64_cuda(5, int(sizes.max()))
     n_str = int(sizes[kinds == "strings"].max()) if (kinds == "strings").any() else 1
-    sd, so = keygen.strings(5, n_str)
-    sdata = torch.from_numpy(sd).cuda()
-    soffs = torch.from_numpy(so.view(np.int64)).cuda()
+    sdata, soffs = keygen.strings_cuda(5, n_str)
     reqs = []
     for t, n, k in zip(times, sizes, kinds):
         n = int(n)
@@ -542,22 +582,38 @@ def run_c5(args) -> None:
     served, s_wall, s_stats, s_failed = replay(4, 0)
     plain, p_wall, p_stats, p_failed = replay(1, 1)
     same = served == plain and not s_failed and not p_failed
-    def summary(wall, st):
-        return {"wall_s": wall, "busy_s": st["busy_ms"] / 1e3, "mkeys_per_s_busy": total / (st["busy_ms"] / 1e3) / 1e6,
-                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
-                "peak_device_bytes": st["peak_bytes"]}
-    print(json.dumps({
-        "workload": "C5 served build stream", "requests": len(reqs), "total_keys": total,
+    del u64_pool, sdata, soffs, reqs
+    torch.cuda.empty_cache()
+
+    def summary(wall, st, failed):
+        return {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                "mkeys_per_s": total / (st["busy_ms"] / 1e3) / 1e6, "busy_s": st["busy_ms"] / 1e3, "wall_s": wall,
+                "peak_device_bytes": st["peak_bytes"], "max_batch_requests": st["max_batch_requests"],
+                "max_batches_in_flight": st["max_batches_in_flight"],
+                "max_device_overlap": st["max_device_overlap"], "failed_by_status": failed}
+
+    return {
+        "workload": f"served build stream, Poisson 200 req/s for {seconds:g} s (seed 5), sizes log-uniform "
+                    f"[1e4, {args.c5_max:.0e}], 70 % u64 / 30 % 8-64-byte strings, lambda 7, P 2048, 120 GB budget",
+        "requests": len(times), "total_keys": total,
         "string_requests": int((kinds == "strings").sum()),
-        "config": {"rate_per_s": 200, "seconds": args.c5_seconds, "sizes": f"log-uniform [1e4, {args.c5_max:.0e}]",
-                   "lambda": lam, "partition_size": P, "budget_gb": 120, "results": "host memory",
-                   "reserved_per_stream": {"device_bytes": reserve[0], "pinned_bytes": reserve[1]},
-                   "keys": "device-resident pools, each request a slice", "data": "synthetic, seed 5"},
-        "served_continuous_batching": {**summary(s_wall, s_stats), "failed_by_status": s_failed},
-        "plain_one_at_a_time": {**summary(p_wall, p_stats), "failed_by_status": p_failed},
+        **summary(s_wall, s_stats, s_failed),
+        "how": "4 streams, continuous batching (phobic_server); results copied to host memory; mkeys_per_s over "
+               "the time with a request in flight",
+        "plain": {**summary(p_wall, p_stats, p_failed), "how": "1 stream, one request per build"},
         "results_identical": same,
-    }), flush=True)
-    if s_failed or p_failed:
+        "reserved_per_stream": {"device_bytes": reserve[0], "pinned_bytes": reserve[1]},
+    }
+
+
+def run_c4(args) -> None:
+    print(json.dumps(c4_leg(args)), flush=True)
+
+
+def run_c5(args) -> None:
+    r = c5_leg(args, args.c5_seconds)
+    print(json.dumps(r), flush=True)
+    if r["failed_by_status"] or r["plain"]["failed_by_status"]:
         sys.exit(1)
 
 
@@ -568,9 +624,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=100_000_000)
-    ap.add_argument("--cpu-sample", type=int, default=20_000_000)
-    ap.add_argument("--ref-sample", type=int, default=20_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched and served legs of the headline line")
+    ap.add_argument("--served-seconds", type=float, default=20.0, help="slice of the request stream in the line")
     ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2")
     ap.add_argument("--c4-sets", type=int, default=4096)
     ap.add_argument("--c5-seconds", type=float, default=60.0)

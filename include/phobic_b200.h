@@ -173,6 +173,26 @@ PHOBIC_API phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *
 PHOBIC_API phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *lines, int reset);
 PHOBIC_API phobic_status phobic_debug_stalled_wait(phobic_ctx *ctx, uint32_t wait_ms, phobic_status *observed);
 
+/* No counterpart in the reference.  Failure injection on the host for the guard against
+ * keys that change during a build: the next build (phobic_build of one set, or
+ * phobic_build_noalloc) of device-visible u64 keys with more than `index` keys runs a
+ * one-thread kernel between its counting pass and its placing pass that does
+ * keys[index] ^= xor_mask on the keys it builds from (the caller's device array, or the
+ * context's staged copy of host keys).  The two passes then disagree and the build must
+ * return PHOBIC_ERR_KEYS_CHANGED.  One shot, process-wide; xor_mask = 0 disarms it. */
+PHOBIC_API phobic_status phobic_debug_change_key(uint64_t index, uint64_t xor_mask);
+
+/* No counterpart in the reference.  Measurement: the integer throughput of the context's
+ * device for the pilot hash's mixing round (x = ((x >> 16) ^ x) * 0x45d9f3b, three 32-bit
+ * operations, hashing.glsl:11-17), many independent chains per thread, every SM at full
+ * occupancy.  *ops_per_s = 32-bit integer operations per second (the denominator of the
+ * search kernel's integer-op roofline), *kernel_ms = the timed kernel's duration. */
+PHOBIC_API phobic_status phobic_measure_int_peak(phobic_ctx *ctx, double *ops_per_s, double *kernel_ms);
+
+/* No counterpart in the reference.  cudaFuncAttributes::binaryVersion of the library's
+ * kernels on the context's device: 100 for code compiled for sm_100a. */
+PHOBIC_API phobic_status phobic_ctx_kernel_arch(phobic_ctx *ctx, int *binary_version);
+
 /* ------------------------------------------------------------------ encoding
  * Mphf::setData (mphf.hpp:65-75) on the host: encodes a build's pilots and
  * partition offsets with the reference's encoders (same bytes as the reference)
@@ -242,13 +262,19 @@ PHOBIC_API phobic_status phobic_debug_build(phobic_ctx *ctx, const phobic_keys *
  *     in at most 65,536 partitions; larger builds return PHOBIC_ERR_BUDGET, other
  *     unsupported inputs PHOBIC_ERR_INVALID.
  *   - result: device arrays (on_device = 1), as for phobic_build.
- *   - stream: the cudaStream_t to run on (NULL = legacy default stream); the call
- *     returns after that stream has drained, with the build's status.
+ *   - stream: the cudaStream_t to run on (NULL = legacy default stream).  The call is
+ *     synchronous: it returns after that stream has drained (waiting at most
+ *     PHOBIC_TIMEOUT_MS, default 120 s), with the build's status.  It must not be made
+ *     while the stream is being captured into a CUDA graph (PHOBIC_ERR_INVALID).
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) for that device; make that first call before any stream
- * capture.  All calls share the array and it keeps the last call's contents (the
- * call clears what must start at zero), so calls whose work overlaps on the GPU
- * race with each other and must not be made. */
+ * (cudaGetSymbolAddress) for that device.  All calls share the array and it keeps
+ * the last call's contents (the call clears what must start at zero).  Calls whose
+ * work would overlap on the GPU would race on the array: while one call's work is
+ * queued or running on a device, other calls on that device return PHOBIC_ERR_BUSY.
+ * After PHOBIC_ERR_TIMEOUT the build's work is still queued on the stream and keeps
+ * the array: later calls on that device return PHOBIC_ERR_BUSY until it has drained,
+ * and the caller must synchronise the stream before it frees or rewrites the keys or
+ * the result arrays. */
 PHOBIC_API phobic_status phobic_build_noalloc(const phobic_keys *keys, const phobic_params *params,
                                               const phobic_result *result, void *stream);
 
@@ -271,6 +297,11 @@ typedef struct phobic_server_stats {
     double p50_ms, p99_ms, max_ms; /* submit-to-completion latency */
     double busy_ms;                /* wall time with at least one request in flight */
     uint64_t peak_bytes;           /* largest admitted device footprint */
+    uint32_t max_batch_requests;   /* most requests built together in one batch */
+    uint32_t max_batches_in_flight;/* most batches queued or running on the device at once */
+    uint32_t max_device_overlap;   /* most batches whose device work (first to last event on
+                                      their streams) overlapped in time */
+    uint32_t pad;
 } phobic_server_stats;
 
 PHOBIC_API phobic_status phobic_server_create(const phobic_server_config *cfg, phobic_server **out);

@@ -68,12 +68,15 @@ uint32_t orc_pilot_hash(uint32_t lower1, uint32_t lower2, uint32_t k);
 
 typedef struct {
     uint64_t hash_evals;    /* hash evaluations made by the search (all k) */
-    uint64_t probe_words;   /* 64-offset windows tested */
+    uint64_t probe_words;   /* 64-offset windows tested (one per window, whatever the bucket size) */
     uint64_t k_retries;     /* pilot-counter increments over all buckets */
     uint32_t max_bucket;    /* largest bucket */
     uint32_t max_partition; /* largest partition */
     uint32_t max_k;         /* largest pilot counter used */
     uint32_t err_partition; /* partition of the first error */
+    uint32_t pad;
+    uint64_t probe_keys;    /* bitmap probes: one 64-bit window of one key's slot (window64 calls);
+                               a window stops taking keys once every offset in it is rejected */
 } orc_stats;
 
 /*

@@ -30,6 +30,8 @@ class Stats(C.Structure):
         ("max_partition", C.c_uint32),
         ("max_k", C.c_uint32),
         ("err_partition", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("probe_keys", C.c_uint64),
     ]
 
 

@@ -164,7 +164,8 @@ static inline void occ_set(uint64_t *occ, uint32_t q, uint32_t ps) {
 
 /* Smallest o in [0, ps) with every (h_i + o) mod ps free (search.comp:72-103
  * under lockstep execution).  Returns ps if there is none. */
-static uint32_t first_offset(const search_ws *ws, uint32_t s, uint32_t ps, int naive, uint64_t *probes) {
+static uint32_t first_offset(const search_ws *ws, uint32_t s, uint32_t ps, int naive, uint64_t *probes,
+                             uint64_t *key_probes) {
     if (naive) {
         for (uint32_t o = 0; o < ps; o++) {
             uint32_t i = 0;
@@ -184,6 +185,7 @@ static uint32_t first_offset(const search_ws *ws, uint32_t s, uint32_t ps, int n
             uint32_t x = ws->h[i] + o0;
             if (x >= ps) x -= ps;
             bad |= window64(ws->occ, x);
+            (*key_probes)++;
         }
         uint64_t valid = ~bad;
         if (ps - o0 < 64) valid &= (1ULL << (ps - o0)) - 1;
@@ -217,7 +219,7 @@ static int search_bucket(search_ws *ws, const uint32_t *l1, const uint32_t *l2, 
             for (uint32_t j = 0; j < i + (i < s); j++) ws->scratch[ws->h[j] >> 6] = 0;
             if (dup) { st->k_retries++; continue; }
         }
-        uint32_t o = first_offset(ws, s, ps, naive, &st->probe_words);
+        uint32_t o = first_offset(ws, s, ps, naive, &st->probe_words, &st->probe_keys);
         if (o < ps) {
             for (uint32_t i = 0; i < s; i++) {
                 uint32_t q = ws->h[i] + o;
@@ -304,9 +306,9 @@ int orc_build(const uint32_t *keys4, uint64_t n, uint32_t P, uint32_t B, const u
 
     int err = ORC_OK;
     uint32_t err_p = 0xFFFFFFFFu;
-    uint64_t tot_hash = 0, tot_probe = 0, tot_retry = 0;
+    uint64_t tot_hash = 0, tot_probe = 0, tot_retry = 0, tot_pkeys = 0;
     uint32_t max_bucket = 0, max_kk = 0;
-#pragma omp parallel num_threads(T) reduction(+ : tot_hash, tot_probe, tot_retry) reduction(max : max_bucket, max_kk)
+#pragma omp parallel num_threads(T) reduction(+ : tot_hash, tot_probe, tot_retry, tot_pkeys) reduction(max : max_bucket, max_kk)
     {
         uint32_t *cnt = (uint32_t *)malloc(B * sizeof(uint32_t));
         uint32_t *in_bin = (uint32_t *)malloc(B * sizeof(uint32_t));
@@ -406,6 +408,7 @@ int orc_build(const uint32_t *keys4, uint64_t n, uint32_t P, uint32_t B, const u
         tot_hash += ls.hash_evals;
         tot_probe += ls.probe_words;
         tot_retry += ls.k_retries;
+        tot_pkeys += ls.probe_keys;
         if (ls.max_k > max_kk) max_kk = ls.max_k;
         free(cnt); free(in_bin); free(bstart); free(fill); free(lperm); free(bpil);
         free(L1); free(L2); free(kb); free(ws.occ); free(ws.scratch); free(ws.h);
@@ -414,6 +417,7 @@ int orc_build(const uint32_t *keys4, uint64_t n, uint32_t P, uint32_t B, const u
     st->hash_evals = tot_hash;
     st->probe_words = tot_probe;
     st->k_retries = tot_retry;
+    st->probe_keys = tot_pkeys;
     st->max_bucket = max_bucket;
     st->max_k = max_kk;
     st->err_partition = err_p;

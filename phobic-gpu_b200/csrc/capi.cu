@@ -278,6 +278,18 @@ phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *line
     return PHOBIC_OK;
 }
 
+phobic_status phobic_measure_int_peak(phobic_ctx *ctx, double *ops_per_s, double *kernel_ms) {
+    if (!ctx || !ops_per_s || !kernel_ms) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return measure_int_peak(ctx->w, ops_per_s, kernel_ms, &ctx->last_error);
+}
+
+phobic_status phobic_ctx_kernel_arch(phobic_ctx *ctx, int *binary_version) {
+    if (!ctx || !binary_version) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return kernel_binary_version(ctx->w.device, binary_version, &ctx->last_error);
+}
+
 phobic_status phobic_verify(phobic_ctx *ctx, const phobic_keys *keys, const phobic_params *params,
                             const phobic_result *built, uint64_t *bad) {
     if (!ctx || !keys || !params || !bad) return PHOBIC_ERR_INVALID;

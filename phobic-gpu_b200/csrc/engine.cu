@@ -19,6 +19,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <thread>
 
 #include <omp.h>
@@ -220,11 +221,15 @@ phobic_status cuda_status(cudaError_t e, const char *what, std::string *err) {
 }
 
 
-phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) {
+// Polls `done` (a cudaEventQuery / cudaStreamQuery) until it succeeds, fails or the
+// bound passes: yields for the first 2000 polls, then sleeps 50 us between polls, so a
+// long build does not hold a host core.
+template <typename Query>
+static phobic_status bounded_wait(Query done, uint64_t timeout_ms, std::string *err) {
     auto t0 = std::chrono::steady_clock::now();
     uint32_t polls = 0;
     for (;;) {
-        cudaError_t e = cudaEventQuery(ev);
+        cudaError_t e = done();
         if (e == cudaSuccess) return PHOBIC_OK;
         if (e != cudaErrorNotReady) return cuda_status(e, "device work failed", err);
         auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
@@ -235,6 +240,45 @@ phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) 
         if (++polls < 2000) std::this_thread::yield();
         else std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err) {
+    return bounded_wait([ev] { return cudaEventQuery(ev); }, timeout_ms, err);
+}
+
+phobic_status wait_stream(cudaStream_t s, uint64_t timeout_ms, std::string *err) {
+    return bounded_wait([s] { return cudaStreamQuery(s); }, timeout_ms, err);
+}
+
+uint64_t env_timeout_ms() {
+    if (const char *t = std::getenv("PHOBIC_TIMEOUT_MS")) {
+        char *end = nullptr;
+        const unsigned long long v = std::strtoull(t, &end, 10);
+        if (end != t && v) return v;
+    }
+    return 120000;
+}
+
+namespace {
+std::mutex g_key_change_mu;
+bool g_key_change_armed = false;
+uint64_t g_key_change_index = 0, g_key_change_mask = 0;
+}  // namespace
+
+void set_key_change(uint64_t index, uint64_t mask) {
+    std::lock_guard<std::mutex> lk(g_key_change_mu);
+    g_key_change_armed = mask != 0;
+    g_key_change_index = index;
+    g_key_change_mask = mask;
+}
+
+bool take_key_change(uint64_t n, int kind, uint64_t *index, uint64_t *mask) {
+    std::lock_guard<std::mutex> lk(g_key_change_mu);
+    if (!g_key_change_armed || kind != PHOBIC_KEYS_U64 || g_key_change_index >= n) return false;
+    g_key_change_armed = false;
+    *index = g_key_change_index;
+    *mask = g_key_change_mask;
+    return true;
 }
 
 uint32_t default_max_partition(uint32_t P) {
@@ -256,7 +300,7 @@ phobic_status Worker::init(int dev, std::string *err) {
     for (auto &e : ev) PHB_TRY(cudaEventCreate(&e), "cudaEventCreate");
     for (auto &e : up_ev) PHB_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     PHB_TRY(pinned.reserve(1 << 16), "cudaMallocHost");
-    if (const char *t = std::getenv("PHOBIC_TIMEOUT_MS")) timeout_ms = std::strtoull(t, nullptr, 10);
+    timeout_ms = env_timeout_ms();
     return PHOBIC_OK;
 }
 
@@ -523,6 +567,9 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         StageRange r("bucket_sizes (K1)");
         PHB_TRY(launch_map_count(kind, ma, plan, s), "K1 map_count");
     }
+    uint64_t kc_index = 0, kc_mask = 0;
+    if (nsets == 1 && take_key_change(N, kind, &kc_index, &kc_mask))
+        PHB_TRY(launch_change_key(const_cast<void *>(hdesc[0].data), kc_index, kc_mask, s), "key change");
     PHB_TRY(cudaEventRecord(w.ev[2], s), "event");
     ScanArgs sa{d_count, d_G, nullptr, (uint32_t)MS, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles), nsets,
                 d_err, 0};

@@ -103,6 +103,18 @@ phobic_status finish_sets(Worker &w, phobic_status *statuses, phobic_timings *t,
 
 // Bounded wait on an event: polls cudaEventQuery until done or timeout.
 phobic_status wait_event(cudaEvent_t ev, uint64_t timeout_ms, std::string *err);
+// The same bounded wait on all work queued on a stream (cudaStreamQuery).
+phobic_status wait_stream(cudaStream_t s, uint64_t timeout_ms, std::string *err);
+// Bound of the host-side waits: PHOBIC_TIMEOUT_MS from the environment, else 120 s.
+uint64_t env_timeout_ms();
+
+// Failure injection on the host (tests of the keys-changed guard): a one-shot request,
+// set by phobic_debug_change_key, to XOR one u64 key with a mask between the counting
+// pass (K1) and the placing pass (K3) of the next build of one set of device-visible
+// u64 keys with more than `index` keys.  Returns true (and clears the request) when
+// this build takes it.
+bool take_key_change(uint64_t n, int kind, uint64_t *index, uint64_t *mask);
+void set_key_change(uint64_t index, uint64_t mask);
 
 phobic_status cuda_status(cudaError_t e, const char *what, std::string *err);
 
@@ -129,6 +141,12 @@ phobic_status run_query(Worker &w, const phobic_keys *keys, const phobic_params 
 // Runs the scan with a never-scheduled first tile (bounded-wait test); *observed gets
 // the status the kernel recorded.
 phobic_status run_stalled_wait(Worker &w, uint32_t wait_ms, phobic_status *observed, std::string *err);
+
+// Measured integer throughput of the device for the pilot hash's mix round (shift, xor,
+// multiply), all SMs at full occupancy: 32-bit operations per second and the kernel time.
+phobic_status measure_int_peak(Worker &w, double *ops_per_s, double *ms, std::string *err);
+// cudaFuncAttributes::binaryVersion of the library's kernels on `device` (100 = sm_100).
+phobic_status kernel_binary_version(int device, int *version, std::string *err);
 
 // Default search bitmap capacity for a partition size (search.comp:21).
 uint32_t default_max_partition(uint32_t partition_size);

@@ -201,6 +201,8 @@ cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st);
 unsigned int check_line_map(bool reset);
 unsigned int check_line_part(bool reset);
 unsigned int check_line_search(bool reset);
+// Failure injection (tests): keys[index] ^= mask, one thread, on stream st.
+cudaError_t launch_change_key(void *keys, uint64_t index, uint64_t mask, cudaStream_t st);
 cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,
                          cudaStream_t st);
 

@@ -97,12 +97,17 @@ __global__ void __launch_bounds__(kMapThreads) k_map(MapArgs a) {
             uint32_t slot[kUnroll];
 #pragma unroll
             for (int u = 0; u < kUnroll; u++)
-                if (gp[u] != 0xFFFFFFFFu) slot[u] = atomicAdd(&a.counts[gp[u]], 1u);
+                if (gp[u] != 0xFFFFFFFFu) slot[u] = PHB_CHECK(gp[u] < a.M) ? atomicAdd(&a.counts[gp[u]], 1u) : 0u;
 #pragma unroll
             for (int u = 0; u < kUnroll; u++) {
                 if (gp[u] == 0xFFFFFFFFu) continue;
-                a.lowers[slot[u]] = make_uint2(l1[u], l2[u]);
-                a.bkt[slot[u]] = (uint16_t)b[u];
+                // A slot at or past the end only comes from keys that changed since K1 counted
+                // them (the search reports PHOBIC_ERR_KEYS_CHANGED): the clamp keeps the store in
+                // the record arrays.
+                const uint64_t at = slot[u] < a.total_keys ? slot[u] : a.total_keys - 1;
+                if (!PHB_CHECK(slot[u] < a.total_keys)) continue;
+                a.lowers[at] = make_uint2(l1[u], l2[u]);
+                a.bkt[at] = (uint16_t)b[u];
             }
         } else {
 #pragma unroll
@@ -255,6 +260,15 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
 }
 
 unsigned int check_line_map(bool reset) { return read_check_line(reset); }
+
+static __global__ void k_change_key(unsigned long long *keys, uint64_t index, unsigned long long mask) {
+    keys[index] ^= mask;
+}
+
+cudaError_t launch_change_key(void *keys, uint64_t index, uint64_t mask, cudaStream_t st) {
+    k_change_key<<<1, 1, 0, st>>>(static_cast<unsigned long long *>(keys), index, mask);
+    return cudaGetLastError();
+}
 
 static size_t chunk_smem(uint64_t partitions, bool narrow) {
     return 4 * ((size_t)kFulcrums + (size_t)(narrow ? (partitions + 1) / 2 : partitions));

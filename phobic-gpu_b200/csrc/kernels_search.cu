@@ -482,8 +482,10 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     const uint16_t *bk = a.bkt + base;
 #pragma unroll 4
     for (uint32_t i = lane; i < ps; i += 32) {
-        const uint32_t b = bk[i];
-        if (PHB_CHECK(b < B)) half_add(ws.cnt32, b);
+        // Ids >= B never come from K3 for keys that K1 counted; the clamp keeps a stale
+        // record (keys changed during the build) inside the tables.
+        const uint32_t b = min((uint32_t)bk[i], B - 1);
+        if (PHB_CHECK(b == bk[i])) half_add(ws.cnt32, b);
     }
     __syncwarp();
 
@@ -552,8 +554,8 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     uint2 *so = a.sorted + base;
 #pragma unroll 4
     for (uint32_t i = lane; i < ps; i += 32) {
-        const uint32_t b = bk[i];
-        if (!PHB_CHECK(b < B)) continue;
+        const uint32_t b = min((uint32_t)bk[i], B - 1);
+        if (!PHB_CHECK(b == bk[i])) continue;
         const uint32_t pos = half_add(ws.cur32, b);
         if (PHB_CHECK(pos < ps)) so[pos] = lo[i];
     }

@@ -14,16 +14,22 @@
 //     the process exits.
 //   * Its device address is looked up once per device with cudaGetSymbolAddress
 //     (host code cannot use the array's name as a device address); the first call
-//     on a device does that lookup, so make the first call on each device before
-//     any stream capture.
+//     on a device does that lookup.
+//   * The call is synchronous: it waits (bounded by PHOBIC_TIMEOUT_MS, default
+//     120 s) for its stream and reads the status.  It copies from host memory and
+//     waits on the stream, so it must not be called while that stream is being
+//     captured into a CUDA graph; such a call returns PHOBIC_ERR_INVALID.
 //   * Every call shares the array and it keeps the previous call's contents: the
 //     counters the kernels need at zero are cleared by each call.  Calls whose
-//     work overlaps on the GPU (on different streams, or from different threads)
-//     race on the array and must not be made.
-#include <chrono>
+//     work would overlap on the GPU race on the array: while one call's work is
+//     queued or running on a device, another call on that device returns
+//     PHOBIC_ERR_BUSY.  A call that returned PHOBIC_ERR_TIMEOUT leaves its work
+//     queued; calls on that device return PHOBIC_ERR_BUSY until that work has
+//     drained, and the caller must synchronise the stream before it frees or
+//     rewrites the keys and result arrays.
+#include <atomic>
 #include <cstring>
 #include <mutex>
-#include <thread>
 
 #include "engine.hpp"
 #include "kernels.cuh"
@@ -57,6 +63,12 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 void *g_scratch_addr[kMaxDevices] = {};
+// 1 while a call's work may use the device's array: set when a call starts, cleared
+// by a host function queued behind that call's last operation (so a call that timed
+// out keeps it set until its work has really finished).
+std::atomic<int> g_in_use[kMaxDevices];
+
+void CUDART_CB release_scratch(void *device) { g_in_use[(intptr_t)device].store(0, std::memory_order_release); }
 
 // Device address of the scratch array on the current device (looked up once).
 phobic_status scratch_address(int device, unsigned char **out) {
@@ -96,6 +108,13 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
     if (!result->partition_offsets || (n && !result->pilots)) return PHOBIC_ERR_INVALID;
     if ((reinterpret_cast<uintptr_t>(result->pilots) | reinterpret_cast<uintptr_t>(result->partition_offsets)) & 3)
         return PHOBIC_ERR_INVALID;
+    cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &capture) != cudaSuccess) {
+        cudaGetLastError();
+        return PHOBIC_ERR_CUDA;
+    }
+    if (capture != cudaStreamCaptureStatusNone) return PHOBIC_ERR_INVALID;  // synchronous: not capturable
 
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) {
@@ -106,7 +125,10 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
     if ((st = scratch_address(device, &base)) != PHOBIC_OK) return st;
     int sm_count = 0;
     if (cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return PHOBIC_ERR_CUDA;
-    cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+    int idle = 0;
+    if (!g_in_use[device].compare_exchange_strong(idle, 1, std::memory_order_acq_rel))
+        return PHOBIC_ERR_BUSY;  // another call's work may still be using the array
+    const uint64_t timeout_ms = env_timeout_ms();
 
     uint32_t *d_fulcs = reinterpret_cast<uint32_t *>(base + kOffFulcs);
     SetDesc *d_desc = reinterpret_cast<SetDesc *>(base + kOffDesc);
@@ -144,6 +166,8 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
     if (ok && m == 0) ok = cuda(cudaMemsetAsync(result->partition_offsets, 0, 4, s));
     if (ok && n) {
         // The global-counter plan: one counter per partition keeps the scratch small.
+        // d_count holds the counts, then (scanned in place) the placement cursors, which
+        // end at the next partition's offset when both passes read the same keys.
         const uint32_t grid = (uint32_t)std::min<uint64_t>((n + kMapThreads - 1) / kMapThreads, (uint64_t)sm_count * 8);
         const MapPlan plan{false, 1, grid, 0};
         MapArgs ma{d_desc, d_kb, 1, B, n, d_fulcs, d_count, nullptr, nullptr, d_lowers, d_bkt, d_err,
@@ -151,26 +175,37 @@ extern "C" phobic_status phobic_build_noalloc(const phobic_keys *keys, const pho
         ScanArgs sa{d_count, d_G, d_count, (uint32_t)m, d_tiles, reinterpret_cast<uint32_t *>(d_tiles + tiles), 1,
                     d_err, 0};
         SearchArgs qa{d_desc, d_pb, 1, (uint32_t)m, d_G, 1, d_lowers, d_bkt, d_sorted, nullptr, B, cap, k_max,
-                      d_queue, d_err};
-        ok = cuda(launch_map_count(keys->kind, ma, plan, s)) && cuda(launch_scan(sa, s)) &&
+                      d_queue, d_err, d_count};
+        uint64_t kc_index = 0, kc_mask = 0;
+        ok = cuda(launch_map_count(keys->kind, ma, plan, s));
+        if (ok && take_key_change(n, keys->kind, &kc_index, &kc_mask))
+            ok = cuda(launch_change_key(const_cast<void *>(keys->data), kc_index, kc_mask, s));
+        ok = ok && cuda(launch_scan(sa, s)) &&
              cuda(launch_check_sizes(d_G, (uint32_t)m, 1, cap, d_pb, 1, d_err, nullptr, s)) &&
              cuda(launch_scatter(keys->kind, ma, plan, s)) && cuda(launch_search(qa, sm_count, s));
     }
-    if (!ok) {
-        cudaGetLastError();
-        return PHOBIC_ERR_CUDA;
+    if (!ok) cudaGetLastError();
+    // Bounded wait for everything queued above (also after a failed launch: work queued
+    // before it may still use the array).
+    st = wait_stream(s, timeout_ms, &err);
+    if (st == PHOBIC_ERR_TIMEOUT) {
+        // The work keeps the array until it drains: release it from the stream then (if
+        // even that cannot be queued, the array stays taken and later calls get BUSY).
+        if (cudaLaunchHostFunc(s, release_scratch, (void *)(intptr_t)device) != cudaSuccess) cudaGetLastError();
+        return st;
     }
-    // Wait (bounded) for the stream, then read the error word.
-    auto t0 = std::chrono::steady_clock::now();
-    for (;;) {
-        cudaError_t e = cudaStreamQuery(s);
-        if (e == cudaSuccess) break;
-        if (e != cudaErrorNotReady) return PHOBIC_ERR_CUDA;
-        if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(120)) return PHOBIC_ERR_TIMEOUT;
-        std::this_thread::yield();
-    }
-    unsigned long long word = 0;
-    if (!cuda(cudaMemcpyAsync(&word, d_err, 8, cudaMemcpyDeviceToHost, s)) || !cuda(cudaStreamSynchronize(s)))
-        return PHOBIC_ERR_CUDA;
+    unsigned long long word = kNoError;
+    // The stream is idle: this copy to pageable memory returns at once.
+    if (st == PHOBIC_OK && ok) ok = cuda(cudaMemcpyAsync(&word, d_err, 8, cudaMemcpyDeviceToHost, s)) &&
+                                    cuda(cudaStreamSynchronize(s));
+    if (!ok) cudaGetLastError();
+    g_in_use[device].store(0, std::memory_order_release);
+    if (st != PHOBIC_OK) return st;
+    if (!ok) return PHOBIC_ERR_CUDA;
     return word == kNoError ? PHOBIC_OK : (phobic_status)(uint32_t)word;
+}
+
+extern "C" phobic_status phobic_debug_change_key(uint64_t index, uint64_t xor_mask) {
+    set_key_change(index, xor_mask);
+    return PHOBIC_OK;
 }

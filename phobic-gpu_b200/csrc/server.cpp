@@ -76,6 +76,10 @@ struct phobic_server {
     double busy_ms = 0;
     int running = 0;
     Clock::time_point busy_since;
+    uint32_t max_batch = 0, max_running = 0;
+    // Device time of each finished batch, in ms after t0_ev: its first event to its last.
+    cudaEvent_t t0_ev = nullptr;
+    std::vector<std::pair<float, float>> device_spans;
 };
 
 namespace {
@@ -111,8 +115,15 @@ void worker_loop(phobic_server *s, StreamWorker *sw) {
         if (e == PHOBIC_OK) e = finish_sets(sw->w, st.data(), nullptr, &err);
         else st.assign(batch.size(), e);
         const auto now = Clock::now();
+        float t_begin = 0.f, t_end = 0.f;
+        const bool timed = e == PHOBIC_OK && s->t0_ev &&
+                           cudaEventElapsedTime(&t_begin, s->t0_ev, sw->w.ev[0]) == cudaSuccess &&
+                           cudaEventElapsedTime(&t_end, s->t0_ev, sw->w.ev[6]) == cudaSuccess;
+        if (!timed) cudaGetLastError();
 
         lk.lock();
+        if (timed) s->device_spans.emplace_back(t_begin, t_end);
+        s->max_batch = std::max<uint32_t>(s->max_batch, (uint32_t)batch.size());
         for (size_t i = 0; i < batch.size(); i++) {
             double ms = std::chrono::duration<double, std::milli>(now - batch[i].submitted).count();
             s->done[batch[i].ticket] = Done{st[i], ms};
@@ -240,6 +251,7 @@ void dispatch_loop(phobic_server *s) {
         free_w->busy = true;
         free_w->batch = std::move(batch);
         if (s->running++ == 0) s->busy_since = Clock::now();
+        s->max_running = std::max<uint32_t>(s->max_running, (uint32_t)s->running);
         s->cv_work.notify_all();
     }
 }
@@ -271,6 +283,13 @@ phobic_status phobic_server_create(const phobic_server_config *cfg, phobic_serve
             return st;
         }
         s->workers.push_back(sw);
+    }
+    // Reference point of the batches' device times (all workers are on one device).
+    if (cudaEventCreate(&s->t0_ev) != cudaSuccess || cudaEventRecord(s->t0_ev, s->workers[0]->w.stream) != cudaSuccess ||
+        cudaEventSynchronize(s->t0_ev) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->t0_ev) cudaEventDestroy(s->t0_ev);
+        s->t0_ev = nullptr;
     }
     for (auto *sw : s->workers) sw->thread = std::thread(worker_loop, s, sw);
     s->dispatcher = std::thread(dispatch_loop, s);
@@ -366,6 +385,19 @@ phobic_status phobic_server_stats_get(phobic_server *s, phobic_server_stats *out
     out->busy_ms = s->busy_ms;
     if (s->running) out->busy_ms += std::chrono::duration<double, std::milli>(Clock::now() - s->busy_since).count();
     out->peak_bytes = s->peak_bytes;
+    out->max_batch_requests = s->max_batch;
+    out->max_batches_in_flight = s->max_running;
+    {
+        // Largest number of device spans covering one instant (a span ending at t does not
+        // overlap one beginning at t).
+        std::vector<std::pair<float, int>> ev;
+        ev.reserve(2 * s->device_spans.size());
+        for (const auto &sp : s->device_spans) ev.emplace_back(sp.first, 1), ev.emplace_back(sp.second, -1);
+        std::sort(ev.begin(), ev.end());
+        int cur = 0, best = 0;
+        for (const auto &e : ev) best = std::max(best, cur += e.second);
+        out->max_device_overlap = (uint32_t)best;
+    }
     if (!s->latencies.empty()) {
         std::vector<double> l = s->latencies;
         std::sort(l.begin(), l.end());
@@ -392,6 +424,7 @@ phobic_status phobic_server_destroy(phobic_server *s) {
         w->w.destroy();
         delete w;
     }
+    if (s->t0_ev) cudaEventDestroy(s->t0_ev);
     delete s;
     return PHOBIC_OK;
 }

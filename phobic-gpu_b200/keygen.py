@@ -5,7 +5,8 @@ No public dataset is involved: every workload is generated from a seed.
     seed, output i is the finalizer of seed + (i+1) * 0x9E3779B97F4A7C15).  It is
     a bijection of the counter, so the keys are unique.
   * strings: lengths uniform in [8, 64], bytes uniform over printable ASCII
-    (0x20..0x7E), duplicates replaced (only short strings can collide).
+    (0x20..0x7E), duplicates replaced (only short strings can collide); a device
+    generator (strings_cuda) of the same distribution serves the request stream.
   * batched sets: sizes log-uniform in [lo, hi].
   * served stream: Poisson arrivals, sizes log-uniform, a u64/string mix.
 """
@@ -89,3 +90,30 @@ def splitmix64_cuda(seed: int, n: int, start: int = 0, device: str = "cuda"):
     z = (z ^ lsr(z, 30)).mul_(s64(int(M1)))
     z = (z ^ lsr(z, 27)).mul_(s64(int(M2)))
     return z ^ lsr(z, 31)
+
+
+def strings_cuda(seed: int, n: int, min_len: int = 8, max_len: int = 64, device: str = "cuda"):
+    """(bytes uint8[total], offsets int64[n+1]) of n strings generated on the device:
+    lengths uniform in [min_len, max_len] and bytes uniform over printable ASCII, both
+    from splitmix64 streams (lengths from seed, bytes from seed ^ 0x5bd1e995, four bytes
+    per output word: 0x20 + (16-bit piece * 95 >> 16)).  Not deduplicated: two strings
+    of 8 printable bytes or more coincide with probability below 1e-4 at 5e7 strings."""
+    import torch
+
+    span = max_len - min_len + 1
+    lens = (splitmix64_cuda(seed, n, device=device) & 0x7FFFFFFF) % span + min_len
+    offs = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    torch.cumsum(lens, 0, out=offs[1:])
+    del lens
+    total = int(offs[-1])
+    data = torch.empty(total, dtype=torch.uint8, device=device)
+    words = (total + 3) // 4
+    chunk = 1 << 26
+    for w0 in range(0, words, chunk):
+        w1 = min(words, w0 + chunk)
+        z = splitmix64_cuda(seed ^ 0x5BD1E995, w1 - w0, start=w0, device=device)
+        pieces = z.view(torch.int16).to(torch.int32) & 0xFFFF  # four 16-bit pieces per word
+        b = (0x20 + ((pieces * 95) >> 16)).to(torch.uint8)
+        lo, hi = 4 * w0, min(total, 4 * w1)
+        data[lo:hi] = b[: hi - lo]
+    return data, offs

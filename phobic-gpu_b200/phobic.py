@@ -94,6 +94,10 @@ class ServerStats(C.Structure):
         ("max_ms", C.c_double),
         ("busy_ms", C.c_double),
         ("peak_bytes", C.c_uint64),
+        ("max_batch_requests", C.c_uint32),
+        ("max_batches_in_flight", C.c_uint32),
+        ("max_device_overlap", C.c_uint32),
+        ("pad", C.c_uint32),
     ]
 
 
@@ -145,6 +149,9 @@ def _lib() -> C.CDLL:
                                     C.POINTER(C.c_size_t), C.POINTER(C.c_double)]),
         "phobic_ctx_result": (I32, [P, U32, U32, C.POINTER(Result)]),
         "phobic_build_noalloc": (I32, [C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), P]),
+        "phobic_debug_change_key": (I32, [U64, U64]),
+        "phobic_measure_int_peak": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+        "phobic_ctx_kernel_arch": (I32, [P, C.POINTER(I32)]),
         "phobic_server_create": (I32, [C.POINTER(ServerConfig), PP]),
         "phobic_server_submit": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_server_poll": (I32, [P, U64, C.POINTER(I32), C.POINTER(I32)]),
@@ -375,6 +382,19 @@ class Context:
         check(_lib().phobic_debug_stalled_wait(self.handle, wait_ms, C.byref(st)), self)
         return int(st.value)
 
+    def int_peak(self) -> tuple[float, float]:
+        """(32-bit integer ops per second, kernel ms) of the pilot hash's mixing round on this
+        device, all SMs at full occupancy (phobic_measure_int_peak)."""
+        ops, ms = C.c_double(), C.c_double()
+        check(_lib().phobic_measure_int_peak(self.handle, C.byref(ops), C.byref(ms)), self)
+        return float(ops.value), float(ms.value)
+
+    def kernel_arch(self) -> int:
+        """cudaFuncAttributes::binaryVersion of the library's kernels (100 = sm_100)."""
+        v = C.c_int()
+        check(_lib().phobic_ctx_kernel_arch(self.handle, C.byref(v)), self)
+        return int(v.value)
+
     def verify(self, keys, cfg: MPHFconfig, built: BuildResult, kind: int | None = None) -> int:
         """Number of keys whose slot is out of range or taken twice (0 = bijection)."""
         ks = keyset(keys, kind)
@@ -384,6 +404,12 @@ class Context:
         k = ks.struct()
         check(_lib().phobic_verify(self.handle, C.byref(k), C.byref(cfg.params), C.byref(res), C.byref(bad)), self)
         return int(bad.value)
+
+
+def debug_change_key(index: int, xor_mask: int) -> None:
+    """Arm phobic_debug_change_key: the next build of one set of device-visible u64 keys
+    flips key `index` by `xor_mask` between its counting and placing passes."""
+    check(_lib().phobic_debug_change_key(index, xor_mask))
 
 
 def _is_cuda(x) -> bool:

@@ -11,7 +11,13 @@ Sources of truth, in order:
     Its pilots are accepted only when the reference's own query maps every key
     to a distinct slot in [0, n).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py              # everything
+    python tests/golden/make_golden.py --full-only  # only the full-size builds (C2, C3, C4)
+
+The full-size builds pin the workloads at the sizes they are quoted on: all 10^8 keys
+of C2, all 5*10^7 strings of C3 and every set of one C4 batch (4096 sets).  Only
+SHA-256 digests are stored; the GPU tests compare element by element with the
+oracle and then with these digests.
 """
 from __future__ import annotations
 
@@ -143,7 +149,52 @@ def build_case(name, keys4, lam, P, keys_u64=None):
     return rec, r
 
 
+def full_size_builds() -> dict:
+    """Oracle builds of the whole C2, C3 and C4 workloads (digests only)."""
+    sys.path.insert(0, str(HERE.parents[1] / "phobic-gpu_b200"))
+    import keygen
+
+    out = {}
+    c2 = O.splitmix64(2, 100_000_000)
+    k4 = ref_keys("u64", c2)
+    rec, r = build_case("C2", k4, 7.0, 2500, c2)
+    out["C2_u64_seed2_n1e8_l7_P2500"] = {k: v for k, v in rec.items() if k not in (
+        "bucket_sizes_sha256", "histo_sha256", "perm_sha256", "sorted_lowers_sha256")}
+    del c2, k4, r
+    sd, so = keygen.strings(3, 50_000_000)
+    k4 = ref_keys("strings", (sd, so))
+    rec, r = build_case("C3", k4, 6.0, 2048)
+    rec.update({"bytes_sha256": sha(sd), "offsets_input_sha256": sha(so)})
+    out["C3_strings_seed3_n5e7_l6_P2048"] = {k: v for k, v in rec.items() if k not in (
+        "bucket_sizes_sha256", "histo_sha256", "perm_sha256", "sorted_lowers_sha256")}
+    del sd, so, k4, r
+    # C4: 4096 sets, one splitmix64(seed 4) stream split in order into sets of sizes
+    # log-uniform in [1e3, 4*2^20]; digests over the sets' pilots (and offsets) in set order.
+    sizes = keygen.set_sizes(4, 4096, 1000, 4 << 20)
+    B, f = O.config(6.0, 2048)
+    hp, ho = hashlib.sha256(), hashlib.sha256()
+    start, max_k = 0, 0
+    for n in sizes:
+        keys = O.splitmix64(4, int(n), start=start)
+        r = O.build(ref_keys("u64", keys), 2048, B, f)
+        assert r["status"] == 0
+        hp.update(np.ascontiguousarray(r["pilots"]).tobytes())
+        ho.update(np.ascontiguousarray(r["offsets"]).tobytes())
+        max_k = max(max_k, int(r["stats"].max_k))
+        start += int(n)
+    out["C4_batch_u64_seed4_4096sets_l6_P2048"] = {
+        "lambda": 6.0, "P": 2048, "buckets": int(B), "sets": len(sizes), "total_keys": int(start),
+        "pilots_concat_sha256": hp.hexdigest(), "offsets_concat_sha256": ho.hexdigest(), "max_k": max_k}
+    return out
+
+
 def main() -> None:
+    if "--full-only" in sys.argv:
+        g = json.loads((HERE / "golden.json").read_text())
+        g["full_builds"] = full_size_builds()
+        (HERE / "golden.json").write_text(json.dumps(g, indent=1))
+        print("updated full_builds in golden.json")
+        return
     if not O.ref_available():
         raise SystemExit("oracle/_ref/libphobic_ref.so missing: make -C oracle (needs the reference checkout)")
     (HERE / "xxh3_vectors.json").write_text(json.dumps(xxh3_vectors(), indent=1))
@@ -198,7 +249,9 @@ def main() -> None:
     builds["C3_sample_strings_seed3_n2e4_l6_P2048"] = rec
 
     np.savez_compressed(HERE / "small_builds.npz", **arrays)
-    (HERE / "golden.json").write_text(json.dumps({"fulcrums": meta, "hashes": hashes, "builds": builds}, indent=1))
+    full = full_size_builds()
+    (HERE / "golden.json").write_text(json.dumps({"fulcrums": meta, "hashes": hashes, "builds": builds,
+                                                  "full_builds": full}, indent=1))
     print("wrote", [p.name for p in HERE.iterdir()])
 
 

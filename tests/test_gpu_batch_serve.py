@@ -66,21 +66,34 @@ def test_batch_reports_per_set_errors(phobic, ctx):
 
 
 def test_server_results_equal_alone(phobic):
+    """Continuous batching: two large requests occupy both streams while 40 small ones
+    arrive; the small ones are built in batches of several requests, two batches are on
+    the device at once, and every result equals the oracle's (and the plain build's)."""
     cfg = phobic.MPHFconfig(7.0, 2048)
     rng = np.random.default_rng(5)
+    big = [keygen.splitmix64(498, 20_000_000), keygen.splitmix64(499, 20_000_000)]
     reqs = []
     for i in range(40):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(3e5))))
         reqs.append(keygen.strings(500 + i, n) if i % 3 == 2 else keygen.splitmix64(500 + i, n))
-    with phobic.Server(0, streams=3, budget_bytes=4 << 30) as srv:
+    with phobic.Server(0, streams=2, budget_bytes=16 << 30) as srv:
+        big_tickets = [srv.submit(k, cfg) for k in big]
         tickets = [srv.submit(k, cfg) for k in reqs]
+        big_results = [srv.wait(t) for t in big_tickets]
         results = [srv.wait(t) for t in tickets]
         stats = srv.stats()
-    assert stats["completed"] == len(reqs) and stats["failed"] == 0
+    assert stats["completed"] == len(reqs) + len(big) and stats["failed"] == 0
     assert stats["p50_ms"] > 0 and stats["p99_ms"] >= stats["p50_ms"]
-    assert stats["peak_bytes"] <= 4 << 30
+    assert stats["peak_bytes"] <= 16 << 30
+    assert stats["max_batch_requests"] > 1, stats     # requests were batched together
+    assert stats["max_batches_in_flight"] > 1, stats  # on more than one stream at once
+    assert stats["max_device_overlap"] > 1, stats     # and their device work overlapped
+    for i, (keys, (st, got)) in enumerate(zip(reqs, results)):
+        assert st == 0
+        want = oracle(O.hash_keys(keys, "strings" if i % 3 == 2 else "u64"), cfg)
+        assert (got.pilots == want["pilots"]).all() and (got.partition_offsets == want["offsets"]).all()
     with phobic.Context(0) as alone:
-        for i, (keys, (st, got)) in enumerate(zip(reqs, results)):
+        for keys, (st, got) in zip(big, big_results):
             assert st == 0
             ref = alone.build(keys, cfg)
             assert (got.pilots == ref.pilots).all() and (got.partition_offsets == ref.partition_offsets).all()

@@ -47,6 +47,11 @@ def check_against_oracle(phobic, ctx, keys, kind, lam, P, debug=True):
     return got
 
 
+def test_kernels_report_sm100(ctx):
+    """cudaFuncGetAttributes: the loaded kernels are sm_100 binaries."""
+    assert ctx.kernel_arch() == 100
+
+
 @pytest.mark.parametrize("n", [0, 1, 2, 31, 2047, 2049, 10000, 100_000])
 def test_u64_small_sizes(phobic, ctx, small_builds, n):
     keys = keygen.splitmix64(1, n)

@@ -52,3 +52,26 @@ def test_memory_limit_gives_oom_and_context_survives(phobic):
         c.set_memory_limit(0)
         got = c.build(keys, cfg)
         assert c.verify(keys, cfg, got) == 0
+
+
+def test_keys_changed_between_passes_is_reported(phobic):
+    """Device keys rewritten between the counting pass and the placing pass (injected from
+    the host by a one-thread kernel on the build's stream) give PHOBIC_ERR_KEYS_CHANGED,
+    with every store kept inside the build's arrays; the context then builds the restored
+    keys correctly."""
+    torch = pytest.importorskip("torch")
+    import numpy as np
+
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(62, 500_000)
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    with phobic.Context(0) as c:
+        phobic.debug_change_key(499_999, 0xFFFF_0000_0000_0000)
+        with pytest.raises(phobic.PhobicError) as e:
+            c.build(dk, cfg)
+        assert e.value.status == phobic.ERR_KEYS_CHANGED
+        dk.copy_(torch.from_numpy(keys.view(np.int64)))  # the injected change, undone
+        got = c.build(dk, cfg)
+        assert c.verify(dk, cfg, got) == 0
+        again = c.build(keys, cfg)
+        assert (again.pilots == got.pilots).all() and (again.partition_offsets == got.partition_offsets).all()

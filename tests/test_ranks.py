@@ -116,7 +116,7 @@ def test_reference_arm_under_two_ranks_prints_once():
         env = dict(os.environ, WORLD_SIZE="2", RANK=str(r), LOCAL_RANK=str(r), MASTER_ADDR="127.0.0.1",
                    MASTER_PORT=str(port))
         outs.append(subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2",
-                                    "--steps", "1", "--warmup", "0", "--ref-sample", "20000"], env=env,
+                                    "--steps", "1", "--warmup", "0", "--n", "20000"], env=env,
                                    capture_output=True, text=True, timeout=300))
     assert all(o.returncode == 0 for o in outs), [o.stderr for o in outs]
     assert outs[1].stdout.strip() == ""
