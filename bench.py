@@ -513,7 +513,7 @@ def c4_leg(args) -> dict:
         "kernel_launches": res[0].timings["kernels"],
         "plain": {"mkeys_per_s": total / seq_wall / 1e6, "wall_ms": 1e3 * seq_wall, "device_ms": seq_dev,
                   "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                  "kernel_launches": 6 * len(sets), "how": "4096 phobic_build calls in sequence, one context"},
+                  "kernel_launches": 6 * len(sizes), "how": "4096 phobic_build calls in sequence, one context"},
         "speedup_vs_plain": seq_wall / batch_wall,
         "all_sets_equal_plain": same, "bijection_bad_sample_of_64": bad,
         "how": "one phobic_build_batch call (wall clock; device_ms from its events), keys and results on the device",

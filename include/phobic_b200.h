@@ -101,10 +101,36 @@ typedef struct phobic_timings {
     uint32_t kernels;         /* kernels launched by the call */
 } phobic_timings;
 
+/* Launch shapes of a context's builds (no counterpart in the reference, whose shapes are
+ * specialisation constants fixed per pipeline, src/search_stage.cpp:36-37). */
+typedef struct phobic_tuning {
+    /* Warps that search one partition together, each trying its own pilot counter per
+     * step (pilots per probe): 1, 2 or 4; 0 = from the autotuner's table when it holds
+     * these parameters, else from the partition count. */
+    uint32_t search_group;
+    uint32_t reserved[7];
+} phobic_tuning;
+
 typedef struct phobic_ctx phobic_ctx;
 typedef struct phobic_server phobic_server;
 
 /* ------------------------------------------------------------------ setup */
+
+/* Sets the launch shapes of the context's later builds (all zero = automatic). */
+PHOBIC_API phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tuning *tuning);
+
+/* No counterpart in the reference (its shapes are per-pipeline specialisation constants,
+ * src/search_stage.cpp:36-37).  Autotuner: builds synthetic u64 keys (splitmix64 on the
+ * device) of 16, 64, 256, 1024, 2048 and 4096 partitions at these parameters with every
+ * search shape (phobic_tuning::search_group 1, 2, 4), and writes the fastest shape per
+ * size class, with the measured build times, to the tab-separated tuning table at path
+ * (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv in the package directory beside the
+ * library's lib/), keeping the table's lines for other devices and parameters.  Builds
+ * with automatic tuning then take their shape from the table: the line of their device,
+ * partition size, bucket count and partition capacity with the smallest size class that
+ * holds their partition count.  *lines_written (optional) = size classes written. */
+PHOBIC_API phobic_status phobic_autotune(phobic_ctx *ctx, const phobic_params *params, const char *path,
+                                         uint32_t *lines_written);
 
 /* Human-readable name of a status code. */
 PHOBIC_API const char *phobic_status_string(phobic_status s);

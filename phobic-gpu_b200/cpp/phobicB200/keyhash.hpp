@@ -165,7 +165,9 @@ PHB_HD H128 len9to16(uint64_t first8, uint64_t last8, uint32_t len) {
 // Hash of a 16-byte input given as two little-endian words.
 PHB_HD H128 hash_16(uint64_t w0, uint64_t w1) { return len9to16(w0, w1, 16); }
 
-// Byte access to an input that may be unaligned.
+// Byte access to an input that may be unaligned.  The hash below reads its input
+// through any type with the same three members (b: one byte, r32 / r64: a little-
+// endian word at any byte offset); the kernels also pass a shared-memory stage.
 struct ByteSrc {
     const uint8_t *p;
     PHB_HD uint8_t b(size_t i) const { return p[i]; }
@@ -181,11 +183,13 @@ struct ByteSrc {
     }
 };
 
-PHB_HD uint64_t mix16(const ByteSrc &s, size_t i, unsigned soff) {
+template <class Src>
+PHB_HD uint64_t mix16(const Src &s, size_t i, unsigned soff) {
     return fold64(s.r64(i) ^ sec64(soff), s.r64(i + 8) ^ sec64(soff + 8));
 }
 
-PHB_HD void mix32(uint64_t &alo, uint64_t &ahi, const ByteSrc &s, size_t a, size_t b, unsigned soff) {
+template <class Src>
+PHB_HD void mix32(uint64_t &alo, uint64_t &ahi, const Src &s, size_t a, size_t b, unsigned soff) {
     alo += mix16(s, a, soff);
     alo ^= s.r64(b) + s.r64(b + 8);
     ahi += mix16(s, b, soff + 16);
@@ -198,7 +202,8 @@ PHB_HD H128 finish_mid(uint64_t alo, uint64_t ahi, size_t len) {
     return H128{avalanche3(lo), 0 - avalanche3(hi)};
 }
 
-PHB_HD void accumulate_stripe(uint64_t acc[8], const ByteSrc &s, size_t i, unsigned soff) {
+template <class Src>
+PHB_HD void accumulate_stripe(uint64_t acc[8], const Src &s, size_t i, unsigned soff) {
     for (int j = 0; j < 8; j++) {
         uint64_t v = s.r64(i + 8 * j);
         uint64_t k = v ^ sec64(soff + 8 * j);
@@ -213,9 +218,9 @@ PHB_HD uint64_t merge(const uint64_t acc[8], unsigned soff, uint64_t start) {
     return avalanche3(r);
 }
 
-// XXH3-128 (seed 0) of an arbitrary byte string.
-PHB_HD H128 hash_bytes(const uint8_t *data, size_t len) {
-    ByteSrc s{data};
+// XXH3-128 (seed 0) of an arbitrary byte string read through s.
+template <class Src>
+PHB_HD H128 hash_src(const Src &s, size_t len) {
     if (len == 0) return H128{avalanche64(sec64(64) ^ sec64(72)), avalanche64(sec64(80) ^ sec64(88))};
     if (len <= 3) {
         uint32_t cl = ((uint32_t)s.b(0) << 16) | ((uint32_t)s.b(len >> 1) << 24) | (uint32_t)s.b(len - 1) |
@@ -269,6 +274,9 @@ PHB_HD H128 hash_bytes(const uint8_t *data, size_t len) {
     accumulate_stripe(acc, s, len - 64, 192 - 64 - 7);
     return H128{merge(acc, 11, (uint64_t)len * kP64_1), merge(acc, 192 - 64 - 11, ~((uint64_t)len * kP64_2))};
 }
+
+// XXH3-128 (seed 0) of an arbitrary byte string.
+PHB_HD H128 hash_bytes(const uint8_t *data, size_t len) { return hash_src(ByteSrc{data}, len); }
 
 }  // namespace xxh3
 

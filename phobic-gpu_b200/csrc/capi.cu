@@ -278,6 +278,21 @@ phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *line
     return PHOBIC_OK;
 }
 
+phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tuning *t) {
+    if (!ctx || !t) return PHOBIC_ERR_INVALID;
+    if (t->search_group != 0 && t->search_group != 1 && t->search_group != 2 && t->search_group != 4)
+        return PHOBIC_ERR_INVALID;
+    ctx->w.search_group = t->search_group;
+    return PHOBIC_OK;
+}
+
+phobic_status phobic_autotune(phobic_ctx *ctx, const phobic_params *params, const char *path,
+                              uint32_t *lines_written) {
+    if (!ctx || !params) return PHOBIC_ERR_INVALID;
+    ctx->last_error.clear();
+    return autotune(ctx->w, params, path, lines_written, &ctx->last_error);
+}
+
 phobic_status phobic_measure_int_peak(phobic_ctx *ctx, double *ops_per_s, double *kernel_ms) {
     if (!ctx || !ops_per_s || !kernel_ms) return PHOBIC_ERR_INVALID;
     ctx->last_error.clear();

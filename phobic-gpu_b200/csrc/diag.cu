@@ -32,7 +32,23 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint32_t iters, uint3
     if (r == 0x2545F491u && seed == 0xFFFFFFFFu) sink[0] = r;
 }
 
+__global__ void k_splitmix(unsigned long long *out, uint64_t n, uint64_t seed) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned long long z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        out[i] = z ^ (z >> 31);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_splitmix(uint64_t *out, uint64_t n, uint64_t seed, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t blocks = std::min<uint64_t>((n + 255) / 256, 148 * 16);
+    k_splitmix<<<(unsigned)blocks, 256, 0, st>>>(reinterpret_cast<unsigned long long *>(out), n, seed);
+    return cudaGetLastError();
+}
 
 phobic_status measure_int_peak(Worker &w, double *ops_per_s, double *ms, std::string *err) {
     PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");

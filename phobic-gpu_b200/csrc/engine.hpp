@@ -74,6 +74,7 @@ struct Worker {
     uint32_t pending_kernels = 0;  // kernels the last enqueued build launched
     unsigned long long *pending_err = nullptr;  // host view of the error words of the last build
     uint64_t timeout_ms = 120000;
+    uint32_t search_group = 0;  // phobic_tuning::search_group (0 = automatic)
 
     phobic_status init(int device, std::string *err);
     void destroy();
@@ -147,6 +148,15 @@ phobic_status run_stalled_wait(Worker &w, uint32_t wait_ms, phobic_status *obser
 phobic_status measure_int_peak(Worker &w, double *ops_per_s, double *ms, std::string *err);
 // cudaFuncAttributes::binaryVersion of the library's kernels on `device` (100 = sm_100).
 phobic_status kernel_binary_version(int device, int *version, std::string *err);
+
+// Warps per partition of the search for a build of `partitions` partitions: the
+// context's setting, else the autotuner's table, else 0 (launch_search's rule).
+uint32_t choose_search_group(const Worker &w, const phobic_params *params, uint32_t partitions);
+// Times the search's launch shapes for a ladder of partition counts at these
+// parameters and writes the fastest per size class to the tuning table at path
+// (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv beside the library's lib/).
+phobic_status autotune(Worker &w, const phobic_params *params, const char *path, uint32_t *lines_written,
+                       std::string *err);
 
 // Default search bitmap capacity for a partition size (search.comp:21).
 uint32_t default_max_partition(uint32_t partition_size);

@@ -195,12 +195,22 @@ cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int 
 // wait on predecessors that never publish: the bounded wait must end in
 // PHOBIC_ERR_TIMEOUT (failure-detection tests).
 cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t st);
-cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st);
+// K4.  group = warps searching one partition together (k-split groups, 2 or 4), 1 = one
+// warp per partition, 0 = chosen from the partition count (search_group_for).
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, int group = 0);
+// Default group size when the autotuner's table has no line for a build: 4 warps per
+// partition when the partitions fill at most a twelfth of the one-warp kernel's warp
+// slots, 2 up to a quarter, else 1.
+int search_group_for(uint32_t partitions, int sm_count);
+size_t search_group_smem(uint32_t buckets, uint32_t cap, int W);
 // First failed bounds check of each kernel file in the checked build (source line, 0 =
 // none; always 0 in the normal build); reset clears it.
 unsigned int check_line_map(bool reset);
 unsigned int check_line_part(bool reset);
 unsigned int check_line_search(bool reset);
+// splitmix64 stream on the device: out[i] = the finalizer of seed + (i + 1) * 0x9E3779B97F4A7C15
+// (synthetic keys of the autotuner).
+cudaError_t launch_splitmix(uint64_t *out, uint64_t n, uint64_t seed, cudaStream_t st);
 // Failure injection (tests): keys[index] ^= mask, one thread, on stream st.
 cudaError_t launch_change_key(void *keys, uint64_t index, uint64_t mask, cudaStream_t st);
 cudaError_t launch_query(int kind, const void *data, const uint64_t *offsets, uint64_t n, const QueryArgs &a, int grid,

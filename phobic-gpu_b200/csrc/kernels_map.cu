@@ -259,6 +259,128 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk(MapArgs a) {
     }
 }
 
+// K1 for string keys, with coalesced loads of the ragged bytes.  A warp takes 32
+// consecutive strings of one set at a time: their bytes are one contiguous span of
+// the set's data, which the warp copies into its shared-memory stage with 16-byte
+// loads (byte loads only for the unaligned head and tail, so no load leaves the
+// span), and each lane then hashes its own string from the stage.  A group whose
+// span does not fit the stage, or whose strings belong to two sets, is hashed from
+// global memory as before.  Counting, the bucket-id check and the {partition,
+// bucket, lower1, lower2} records for K3 are those of k_chunk.
+constexpr uint32_t kStrStageBytes = 2304;  // per warp: 32 strings of up to 64 bytes, with slack
+constexpr uint32_t kStrStageSlack = 32;    // alignment (<= 15 bytes) and the stage reads' overhang (<= 12)
+
+// The stage as a byte source for the hash: bytes [start, start + len) of the warp's
+// stage, read with 32-bit shared-memory loads and funnel shifts.
+struct StageSrc {
+    uint32_t sa;     // shared-space byte address of the stage
+    uint32_t start;  // the string's first byte inside the stage
+
+    __device__ __forceinline__ uint32_t word(uint32_t k) const {
+        uint32_t v;
+        asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(sa + 4 * k));
+        return v;
+    }
+    __device__ __forceinline__ uint8_t b(size_t i) const {
+        const uint32_t x = start + (uint32_t)i;
+        return (uint8_t)(word(x >> 2) >> ((x & 3) * 8));
+    }
+    __device__ __forceinline__ uint32_t r32(size_t i) const {
+        const uint32_t x = start + (uint32_t)i, k = x >> 2, sh = (x & 3) * 8;
+        return __funnelshift_r(word(k), word(k + 1), sh);
+    }
+    __device__ __forceinline__ uint64_t r64(size_t i) const {
+        const uint32_t x = start + (uint32_t)i, k = x >> 2, sh = (x & 3) * 8;
+        const uint32_t w0 = word(k), w1 = word(k + 1), w2 = word(k + 2);
+        return (uint64_t)__funnelshift_r(w0, w1, sh) | ((uint64_t)__funnelshift_r(w1, w2, sh) << 32);
+    }
+};
+
+template <bool NARROW>
+__global__ void __launch_bounds__(kChunkThreads, 1) k_chunk_str(MapArgs a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t wrapped;
+    uint32_t *sf = smem;               // [kFulcrums]
+    uint32_t *cnt = smem + kFulcrums;  // [M], or [(M + 1) / 2] packed
+    const uint32_t words = NARROW ? (a.M + 1) / 2 : a.M;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *stage = smem + ((kFulcrums + words + 3) & ~3u) + (size_t)warp * (kStrStageBytes / 4);
+    const uint32_t stage_sa = (uint32_t)__cvta_generic_to_shared(stage);
+    char *stage_b = reinterpret_cast<char *>(stage);
+    const uint32_t c = blockIdx.x;
+    for (uint32_t i = threadIdx.x; i < kFulcrums; i += blockDim.x) sf[i] = a.fulcs[i];
+    for (uint32_t g = threadIdx.x; g < words; g += blockDim.x) cnt[g] = 0u;
+    if (threadIdx.x == 0) wrapped = 0u;
+    __syncthreads();
+
+    const uint64_t lo = (uint64_t)c * a.chunk;
+    const uint64_t hi = lo + a.chunk < a.total_keys ? lo + a.chunk : a.total_keys;
+    SetCache sc;
+    uint32_t bad_set = 0xFFFFFFFFu;
+    for (uint64_t gbase = lo + 32 * (uint64_t)warp; gbase < hi; gbase += 32 * (uint64_t)(kChunkThreads / 32)) {
+        const uint64_t g = gbase + lane;
+        const bool valid = g < hi;
+        uint64_t a_off = 0, b_off = 0;
+        if (valid) {
+            sc.locate(a, g);
+            a_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo));
+            b_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo) + 1);
+        }
+        const uint32_t vmask = __ballot_sync(kFullMask, valid);
+        const int last = 31 - __clz(vmask);
+        const unsigned long long data0 = __shfl_sync(kFullMask, (unsigned long long)sc.data, 0);
+        const bool one_set = __all_sync(kFullMask, !valid || (unsigned long long)sc.data == data0);
+        const uint64_t span_lo = __shfl_sync(kFullMask, a_off, 0), span_hi = __shfl_sync(kFullMask, b_off, last);
+        Key4 k{};
+        if (one_set && span_hi >= span_lo && span_hi - span_lo <= kStrStageBytes - kStrStageSlack) {
+            const uint64_t A = data0 + span_lo, E = data0 + span_hi;
+            const uint64_t A0 = A & ~15ull, A16 = (A + 15) & ~15ull, E16 = E & ~15ull;
+            // Interior 16-byte blocks, then the head [A, min(A16, E)) and the tail
+            // [max(E16, A16), E): every load lies inside [A, E).
+            for (uint64_t q = A16 + 16 * (uint64_t)lane; q + 16 <= E16; q += 512)
+                *reinterpret_cast<uint4 *>(stage_b + (q - A0)) = __ldg(reinterpret_cast<const uint4 *>(q));
+            const uint64_t head_end = A16 < E ? A16 : E, tail_begin = E16 > A16 ? E16 : A16;
+            if (A + lane < head_end) stage_b[A + lane - A0] = (char)__ldg(reinterpret_cast<const unsigned char *>(A + lane));
+            if (tail_begin + lane < E)
+                stage_b[tail_begin + lane - A0] = (char)__ldg(reinterpret_cast<const unsigned char *>(tail_begin + lane));
+            __syncwarp();
+            if (valid)
+                k = key_from_hash(xxh3::hash_src(StageSrc{stage_sa, (uint32_t)(A - A0 + (a_off - span_lo))},
+                                                 (size_t)(b_off - a_off)));
+            __syncwarp();
+        } else if (valid) {
+            k = key_from_hash(xxh3::hash_bytes(static_cast<const uint8_t *>(sc.data) + a_off, (size_t)(b_off - a_off)));
+        }
+        if (!valid) continue;
+        const uint32_t gp = sc.part_base + partition_of(k.partitioner, sc.partitions);
+        const uint32_t b = bucket_of(k.bucketer, sf);
+        if (b >= a.buckets && bad_set == 0xFFFFFFFFu) bad_set = sc.s;
+        if (a.debug_keys) a.debug_keys[g] = make_uint4(k.partitioner, k.bucketer, k.lower1, k.lower2);
+        a.mapped[g] = make_uint4(gp, b, k.lower1, k.lower2);
+        if (!PHB_CHECK(gp < a.M)) continue;
+        if (NARROW) {
+            const uint32_t old = atomicAdd(&cnt[gp >> 1], 1u << ((gp & 1u) << 4));
+            if (((old >> ((gp & 1u) << 4)) & 0xFFFFu) == 0xFFFFu) credit_wrap(a, c, gp, old, &wrapped);
+        } else {
+            atomicAdd(&cnt[gp], 1u);
+        }
+    }
+    if (bad_set != 0xFFFFFFFFu) report_error(&a.err[bad_set], 0, PHOBIC_ERR_INVALID);
+    __syncthreads();
+    if (NARROW) {
+        const bool add = wrapped != 0u;
+        for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) {
+            const uint32_t v = (cnt[g >> 1] >> ((g & 1u) << 4)) & 0xFFFFu;
+            if (add)
+                atomicAdd(&a.counts[(size_t)g * a.stride + c], v);
+            else
+                a.counts[(size_t)g * a.stride + c] = v;
+        }
+    } else {
+        for (uint32_t g = threadIdx.x; g < a.M; g += blockDim.x) a.counts[(size_t)g * a.stride + c] = cnt[g];
+    }
+}
+
 unsigned int check_line_map(bool reset) { return read_check_line(reset); }
 
 static __global__ void k_change_key(unsigned long long *keys, uint64_t index, unsigned long long mask) {
@@ -295,8 +417,23 @@ MapPlan plan_map(uint64_t total_keys, uint64_t partitions, int sm_count) {
     return p;
 }
 
+// Shared memory of k_chunk_str: the counters, then one stage per warp.
+static size_t chunk_str_smem(uint64_t partitions, bool narrow) {
+    const size_t words = (size_t)kFulcrums + (size_t)(narrow ? (partitions + 1) / 2 : partitions);
+    return 4 * ((words + 3) & ~size_t(3)) + (size_t)(kChunkThreads / 32) * kStrStageBytes;
+}
+
 template <int KIND, bool SCATTER, bool NARROW>
 static cudaError_t launch_chunk(const MapArgs &a, const MapPlan &plan, cudaStream_t st) {
+    if constexpr (KIND == PHOBIC_KEYS_STRINGS && !SCATTER) {
+        // Staged string loads whenever the stages fit beside the counters.
+        const size_t smem = chunk_str_smem(a.M, NARROW);
+        if (allow_dynamic_smem(k_chunk_str<NARROW>, smem) == cudaSuccess) {
+            k_chunk_str<NARROW><<<plan.grid, kChunkThreads, smem, st>>>(a);
+            return cudaSuccess;
+        }
+        cudaGetLastError();
+    }
     const size_t smem = chunk_smem(a.M, NARROW);
     cudaError_t e = allow_dynamic_smem(k_chunk<KIND, SCATTER, NARROW>, smem);
     if (e != cudaSuccess) return e;

@@ -456,9 +456,14 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
     return PHOBIC_ERR_SEARCH_LIMIT;
 }
 
-// One partition: bucket histogram, search order, bucket-sorted keys, pilots.
-__device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
-                                                     uint32_t g, uint32_t p, int lane) {
+// Preparation of one partition by one warp: bucket histogram, search order (in
+// ws.sched), bucket-ordered keys (in a.sorted), pilot 0 for empty buckets, a clear
+// bitmap and collision scratch.  *nonempty = buckets to search; *skip = true when the
+// partition is not searched here (reported by the size check).  Returns a status.
+__device__ __forceinline__ uint32_t prep_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
+                                                   uint32_t g, uint32_t p, int lane, uint32_t *nonempty_out,
+                                                   bool *skip) {
+    *skip = true;
     const uint32_t B = a.buckets;
     const uint32_t base = a.G[(size_t)g * a.gstride];
     const uint32_t end = a.G[(size_t)(g + 1) * a.gstride];
@@ -468,6 +473,7 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     const uint32_t ps = end - base;
     if (ps > a.cap) return PHOBIC_OK;  // reported by the size check
     if (!PHB_CHECK(base + ps <= a.G[(size_t)a.M * a.gstride])) return PHOBIC_OK;
+    *skip = false;
     if (placed != end) return PHOBIC_ERR_KEYS_CHANGED;
     const uint32_t ow = bitmap_words(a.cap);
     uint32_t *pil = d.pilots + p;
@@ -564,6 +570,23 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
     // The search-phase half of the union: large buckets expect a clear collision scratch.
     for (uint32_t i = lane; i < scr_words(a.cap); i += 32) ws.scr[i] = 0;
     __syncwarp();
+    *nonempty_out = nonempty;
+    return PHOBIC_OK;
+}
+
+// One partition: bucket histogram, search order, bucket-sorted keys, pilots.
+__device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
+                                                     uint32_t g, uint32_t p, int lane) {
+    uint32_t nonempty = 0;
+    bool skip = true;
+    const uint32_t pst = prep_partition(a, ws, d, g, p, lane, &nonempty, &skip);
+    if (skip || pst != PHOBIC_OK) return pst;
+    const uint32_t B = a.buckets;
+    const uint32_t base = a.G[(size_t)g * a.gstride];
+    const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
+    uint32_t *pil = d.pilots + p;
+    const size_t pstride = d.partitions;
+    const uint2 *so = a.sorted + base;
 
     // Pilot search (search.comp:126-175), next bucket's keys prefetched.
     const FastMod fm = FastMod::make(ps ? ps : 1);
@@ -590,6 +613,228 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         if (lane == 0 && PHB_CHECK(b < B)) pil[(size_t)b * pstride] = pilot;
     }
     return PHOBIC_OK;
+}
+
+// ------------------------------------------------------------------ k-split groups
+//
+// For builds with far fewer partitions than warp slots (small key sets, where one
+// warp per partition leaves most of the GPU idle and each partition's search is
+// bound by the latency of its sequential tries), a group of W warps searches one
+// partition: in each step, warp w tries pilot counter k0 + w for the current bucket
+// (hash, collision test, offset scan over all of [0, ps)).  The step's outcomes are
+// exchanged in shared memory and read in k order, so the bucket takes the smallest k
+// that has a free offset, with that k's smallest offset: the result of trying
+// k = 0, 1, 2, ... one at a time (search.comp:105-124).  Every warp then marks the
+// winning slots itself (the marks are idempotent), so no warp reads the bitmap before
+// its own copy of the marks is in place.
+constexpr uint32_t kTryNone = 0, kTryFound = 1, kTryDup = 2, kTryLimit = 3;
+
+__device__ __forceinline__ void group_bar(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// Per-warp scratch of warps 1..W-1 of a group (warp 0 uses the union of carve()).
+__host__ __device__ __forceinline__ size_t group_extra_words(uint32_t cap) {
+    return ((size_t)kHsWords + scr_words(cap) + 3) & ~size_t(3);
+}
+// Exchange words: [2 parities][W] outcomes, then the job and status words (padded).
+__host__ __device__ __forceinline__ size_t group_xch_words(int W) { return ((size_t)2 * W + 4 + 3) & ~size_t(3); }
+__host__ __device__ __forceinline__ size_t group_words(uint32_t B, uint32_t cap, int W) {
+    return warp_words(B, cap) + (size_t)(W - 1) * group_extra_words(cap) + group_xch_words(W);
+}
+
+// One try of pilot counter k for a bucket of s <= 32 keys (key `lane` in L): the
+// collision test and offset scan of place_small.  kTryFound with *o, else kTryNone.
+__device__ __forceinline__ uint32_t try_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
+                                              uint32_t k, uint32_t rounds, int lane, uint32_t *o_out) {
+    const bool mine = lane < (int)s;
+    const uint32_t padded = (s + 3) & ~3u;
+    const uint32_t h = mine ? fm.mod(pilot_hash(L.x, L.y, k)) : (0x80000000u | lane);
+    if (s > 1) {
+        uint32_t m = __match_any_sync(kFullMask, h);
+        if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) return kTryNone;
+    }
+    const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
+    uint32_t o;
+    if (s <= 8 && rounds <= 3) {
+        if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
+        else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
+    } else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
+    else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
+    else {
+        if (lane < (int)padded) ws.hs[lane] = hp;
+        __syncwarp();
+        o = first_free_offset(ws.occ, ws.hs, s, ps, lane, ws.occ_lo, ws.occ_hi);
+        __syncwarp();
+    }
+    if (o == kNone) return kTryNone;
+    *o_out = o;
+    return kTryFound;
+}
+
+// One try of pilot counter k for a bucket of more than 32 keys read from src: the
+// chunked collision test and offset scan of place_large.
+__device__ __forceinline__ uint32_t try_large(const WarpSmem &ws, const uint2 *src, uint32_t s, uint32_t ps,
+                                              FastMod fm, uint32_t k, int lane, uint32_t *o_out) {
+    const uint32_t padded = (s + 3) & ~3u;
+    bool dup = false;
+    uint32_t done = 0;
+    for (uint32_t c0 = 0; c0 < s && !dup; c0 += 32) {
+        const uint32_t i = c0 + lane;
+        bool d = false;
+        if (i < s) {
+            const uint2 key = src[i];
+            const uint32_t h = fm.mod(pilot_hash(key.x, key.y, k));
+            ws.hs[i] = pack_slot(h);
+            const uint32_t bit = 1u << (h & 31);
+            d = PHB_CHECK(h < ps) && (atomicOr(&ws.scr[h >> 5], bit) & bit) != 0;
+        }
+        dup = __any_sync(kFullMask, d);
+        done = c0 + 32;
+    }
+    for (uint32_t i = lane; i < s && i < done; i += 32) ws.scr[unpack_slot(ws.hs[i]) >> 5] = 0;
+    __syncwarp();
+    if (dup) return kTryNone;
+    if (s + lane < padded) ws.hs[s + lane] = ws.hs[0];
+    __syncwarp();
+    const uint32_t o = first_free_offset(ws.occ, ws.hs, s, ps, lane, ws.occ_lo, ws.occ_hi);
+    __syncwarp();
+    if (o == kNone) return kTryNone;
+    *o_out = o;
+    return kTryFound;
+}
+
+// Whether two of the s keys read from src are identical (the check at pilot counter
+// kDupCheckAt of place_large).
+__device__ __noinline__ bool has_duplicate_key_src(const uint2 *src, uint32_t s, int lane) {
+    bool d = false;
+    for (uint32_t t = 0; t + 1 < s; t++) {
+        const uint2 kt = src[t];
+        for (uint32_t i = lane; i < s; i += 32) d |= i > t && src[i].x == kt.x && src[i].y == kt.y;
+    }
+    return __any_sync(kFullMask, d);
+}
+
+// Marks the slots (h_i + o) mod ps of the bucket's keys at pilot counter k.
+__device__ __forceinline__ void mark_bucket(const WarpSmem &ws, uint2 L, const uint2 *src, uint32_t s, uint32_t ps,
+                                            FastMod fm, uint32_t k, uint32_t o, int lane) {
+    if (s <= 32) {
+        if (lane < (int)s) {
+            uint32_t q = fm.mod(pilot_hash(L.x, L.y, k)) + o;
+            q = q >= ps ? q - ps : q;
+            if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
+        }
+    } else {
+        for (uint32_t i = lane; i < s; i += 32) {
+            const uint2 key = src[i];
+            uint32_t q = fm.mod(pilot_hash(key.x, key.y, k)) + o;
+            q = q >= ps ? q - ps : q;
+            if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
+        }
+    }
+    __syncwarp();
+}
+
+// Group kernel: kSearchWarps / W groups per CTA, each a persistent searcher over the
+// partition queue.  Warp 0 of a group prepares the partition (prep_partition); all W
+// warps then search its buckets in k-split steps.
+// Small builds leave most SMs idle, so the group kernel is not held to the one-warp
+// kernel's 4 CTAs per SM (64 registers): 2 CTAs per SM keep it free of spills.
+template <int W>
+__global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArgs a) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int grp = warp / W, w = warp % W;
+    const uint32_t bar_id = 1 + grp, bar_n = 32 * W;
+    uint32_t *gbase = smem + (size_t)grp * group_words(a.buckets, a.cap, W);
+    WarpSmem ws = carve(gbase, a.buckets, a.cap);
+    if (w > 0) {
+        ws.hs = gbase + warp_words(a.buckets, a.cap) + (size_t)(w - 1) * group_extra_words(a.cap);
+        ws.scr = ws.hs + kHsWords;
+    }
+    uint32_t *xch = gbase + warp_words(a.buckets, a.cap) + (size_t)(W - 1) * group_extra_words(a.cap);
+    uint32_t *ctl = xch + 2 * W;  // [0] job, [1] status / nonempty
+    uint32_t par = 0;
+    for (;;) {
+        if (w == 0 && lane == 0) ctl[0] = atomicAdd(a.queue, 1u);
+        group_bar(bar_id, bar_n);
+        const uint32_t g = ctl[0];
+        if (g >= a.M) break;
+        const uint32_t s_idx = a.nsets == 1 ? 0u : find_set(a.part_base, a.nsets, g);
+        const SetDesc &d = a.sets[s_idx];
+        const uint32_t p = g - d.part_base;
+        // Warp 0 prepares; ctl[1] = nonempty buckets, or 0xFFFFFFFF when there is nothing to search.
+        if (w == 0) {
+            uint32_t ctl1 = 0xFFFFFFFFu;
+            if (!fatal_before_search(*reinterpret_cast<volatile unsigned long long *>(&a.err[s_idx]))) {
+                if (lane == 0 && d.part_off) {
+                    const uint32_t g0 = a.G[(size_t)d.part_base * a.gstride];
+                    d.part_off[p] = a.G[(size_t)g * a.gstride] - g0;
+                    if (p + 1 == d.partitions) d.part_off[p + 1] = a.G[(size_t)(g + 1) * a.gstride] - g0;
+                }
+                uint32_t nonempty = 0;
+                bool skip = true;
+                const uint32_t code = prep_partition(a, ws, d, g, p, lane, &nonempty, &skip);
+                if (code != PHOBIC_OK && lane == 0) report_error(&a.err[s_idx], p, code);
+                if (!skip && code == PHOBIC_OK) ctl1 = nonempty;
+            }
+            if (lane == 0) ctl[1] = ctl1;
+        } else {
+            for (uint32_t i = lane; i < scr_words(a.cap); i += 32) ws.scr[i] = 0;
+        }
+        group_bar(bar_id, bar_n);
+        const uint32_t nonempty = ctl[1];
+        if (nonempty != 0xFFFFFFFFu) {
+            const uint32_t base = a.G[(size_t)g * a.gstride];
+            const uint32_t ps = a.G[(size_t)(g + 1) * a.gstride] - base;
+            const uint2 *so = a.sorted + base;
+            uint32_t *pil = d.pilots + p;
+            const size_t pstride = d.partitions;
+            const FastMod fm = FastMod::make(ps ? ps : 1);
+            const uint32_t rounds = (ps + 1023) / 1024;
+            uint32_t k_lim = 0x80000000u / (ps ? ps : 1);
+            if (k_lim > a.k_max) k_lim = a.k_max;
+            uint32_t err = PHOBIC_OK;
+            for (uint32_t j = 0; j < nonempty && err == PHOBIC_OK; j++) {
+                const uint32_t sc = ws.sched[j];
+                const uint32_t b = sc >> 16, st = sc & 0xFFFFu;
+                const uint32_t s = half_get(ws.cnt32, b);
+                const uint2 *src = so + st;
+                const uint2 L = lane < (int)s && s <= 32 ? src[lane] : make_uint2(0, 0);
+                for (uint32_t k0 = 0;; k0 += W) {
+                    const uint32_t k = k0 + w;
+                    uint32_t code = kTryNone, o = 0;
+                    if (k >= k_lim) code = kTryLimit;
+                    else if (k == kDupCheckAt && s > 1 &&
+                             (s <= 32 ? has_duplicate_key(L, s, lane) : has_duplicate_key_src(src, s, lane)))
+                        code = kTryDup;
+                    else code = s <= 32 ? try_small(ws, L, s, ps, fm, k, rounds, lane, &o)
+                                        : try_large(ws, src, s, ps, fm, k, lane, &o);
+                    if (lane == 0) xch[par * W + w] = (code << 16) | (o & 0xFFFFu);
+                    group_bar(bar_id, bar_n);
+                    uint32_t win = kTryNone << 16, v = 0;
+                    for (; v < (uint32_t)W; v++) {
+                        win = xch[par * W + v];
+                        if ((win >> 16) != kTryNone) break;
+                    }
+                    par ^= 1u;
+                    const uint32_t wcode = win >> 16;
+                    if (wcode == kTryNone) continue;
+                    if (wcode == kTryFound) {
+                        const uint32_t kw = k0 + v, ow = win & 0xFFFFu;
+                        mark_bucket(ws, L, src, s, ps, fm, kw, ow, lane);
+                        if (w == 0 && lane == 0 && PHB_CHECK(b < a.buckets)) pil[(size_t)b * pstride] = ow + ps * kw;
+                    } else {
+                        err = wcode == kTryDup ? PHOBIC_ERR_DUPLICATE_KEY : PHOBIC_ERR_SEARCH_LIMIT;
+                    }
+                    break;
+                }
+            }
+            if (err != PHOBIC_OK && w == 0 && lane == 0) report_error(&a.err[s_idx], p, err);
+        }
+        // Everyone is done with this partition's tables before warp 0 fetches and prepares the next.
+        group_bar(bar_id, bar_n);
+    }
 }
 
 }  // namespace
@@ -627,8 +872,43 @@ __global__ void __launch_bounds__(kSearchWarps * 32, kSearchCtasPerSm) k_search(
     }
 }
 
-cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st) {
+size_t search_group_smem(uint32_t buckets, uint32_t cap, int W) { return 4 * group_words(buckets, cap, W); }
+
+template <int W>
+static cudaError_t launch_group(const SearchArgs &a, int sm_count, cudaStream_t st) {
+    constexpr int groups = kSearchWarps / W;
+    const size_t smem = (size_t)groups * search_group_smem(a.buckets, a.cap, W);
+    if (smem > kSearchSmemLimit) return cudaErrorInvalidValue;
+    cudaError_t e = allow_dynamic_smem(k_search_group<W>, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search_group<W>, kSearchWarps * 32, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    const uint64_t want = (a.M + groups - 1) / groups;
+    const int grid = (int)std::min<uint64_t>(want, (uint64_t)per_sm * sm_count);
+    k_search_group<W><<<grid, kSearchWarps * 32, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+int search_group_for(uint32_t partitions, int sm_count) {
+    // Warp slots of the one-warp kernel: kSearchWarps * kSearchCtasPerSm per SM (4736 on a
+    // B200).  Measured on a B200 (the autotuner's ladder at six parameter sets): groups of 4
+    // are fastest up to about 256 partitions, groups of 2 around 1024, one warp from 2048 on.
+    const uint64_t slots = (uint64_t)(sm_count > 0 ? sm_count : 148) * kSearchWarps * kSearchCtasPerSm;
+    if ((uint64_t)partitions * 12 <= slots) return 4;
+    if ((uint64_t)partitions * 4 <= slots) return 2;
+    return 1;
+}
+
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, int group) {
     if (a.M == 0) return cudaSuccess;
+    if (group == 0) group = search_group_for(a.M, sm_count);
+    if (group == 2 || group == 4) {
+        cudaError_t e = group == 2 ? launch_group<2>(a, sm_count, st) : launch_group<4>(a, sm_count, st);
+        if (e != cudaErrorInvalidValue) return e;
+        cudaGetLastError();  // the group's tables do not fit: one warp per partition
+    }
     const int warps = search_warps_per_cta(a.buckets, a.cap);
     if (warps < 1) return cudaErrorInvalidValue;
     const size_t smem = (size_t)warps * search_warp_smem(a.buckets, a.cap);

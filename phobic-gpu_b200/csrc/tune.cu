@@ -1,0 +1,233 @@
+// The search's launch-shape table and the autotuner that fills it.
+//
+// The reference fixes its launch shapes per pipeline as specialisation constants
+// (src/search_stage.cpp:36-37, include/phobicGpu/mphf_builder.h:39-45).  Here the
+// shape that matters across workload sizes is the number of warps searching one
+// partition together (each warp trying its own pilot counter per step, so also the
+// pilots tried per probe): one warp per partition when the partitions fill the GPU,
+// groups of 2 or 4 when a build has few partitions and each partition's search is
+// bound by the latency of its sequential tries.
+//
+// phobic_autotune times every shape on synthetic keys (splitmix64 on the device) for a
+// ladder of partition counts at the caller's parameters, and records the fastest
+// per (device name, P, B, partition capacity, size class) as one line of a tab-
+// separated table:
+//     device  partition_size  buckets  max_partition_size  max_partitions  search_group  [ms per shape...]
+// A build looks its shape up in that table (the first line of its device and
+// parameters whose max_partitions is >= its partition count); builds larger than
+// every class, or without a line, use the partition-count rule of launch_search.
+// The table is read from $PHOBIC_TUNING_FILE, else from tuning.tsv in the package
+// directory beside the library (lib/..).
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "engine.hpp"
+#include "kernels.cuh"
+
+namespace phobicb200 {
+namespace {
+
+struct TuneLine {
+    std::string device;
+    uint32_t P, B, cap, max_parts, group;
+};
+
+std::mutex g_tune_mu;
+bool g_tune_loaded = false;
+std::vector<TuneLine> g_tune;
+
+std::string default_table_path() {
+    if (const char *p = std::getenv("PHOBIC_TUNING_FILE")) return p;
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void *>(&default_table_path), &info) && info.dli_fname) {
+        std::string lib = info.dli_fname;  // <package>/lib/libphobic_b200.so
+        const size_t cut = lib.rfind('/');
+        if (cut != std::string::npos) {
+            const std::string dir = lib.substr(0, cut);
+            const size_t up = dir.rfind('/');
+            return (up == std::string::npos ? std::string(".") : dir.substr(0, up)) + "/tuning.tsv";
+        }
+    }
+    return "tuning.tsv";
+}
+
+std::vector<TuneLine> parse_lines(std::istream &f) {
+    std::vector<TuneLine> out;
+    std::string line;
+    while (std::getline(f, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::vector<std::string> col;
+        std::stringstream ss(line);
+        std::string c;
+        while (std::getline(ss, c, '\t')) col.push_back(c);
+        if (col.size() < 6) continue;
+        TuneLine t;
+        t.device = col[0];
+        t.P = (uint32_t)std::strtoul(col[1].c_str(), nullptr, 10);
+        t.B = (uint32_t)std::strtoul(col[2].c_str(), nullptr, 10);
+        t.cap = (uint32_t)std::strtoul(col[3].c_str(), nullptr, 10);
+        t.max_parts = (uint32_t)std::strtoul(col[4].c_str(), nullptr, 10);
+        t.group = (uint32_t)std::strtoul(col[5].c_str(), nullptr, 10);
+        if (t.group == 1 || t.group == 2 || t.group == 4) out.push_back(t);
+    }
+    return out;
+}
+
+std::vector<TuneLine> parse_table(const std::string &path) {
+    std::ifstream f(path);
+    return parse_lines(f);
+}
+
+std::vector<TuneLine> parse_table_text(const std::string &text) {
+    std::istringstream f(text);
+    return parse_lines(f);
+}
+
+// Whether a table line is for this device and these parameters.
+bool parse_table_line_matches(const std::string &line, const std::string &dev, uint32_t P, uint32_t B, uint32_t cap) {
+    const std::vector<TuneLine> one = parse_table_text(line);
+    return !one.empty() && one[0].device == dev && one[0].P == P && one[0].B == B && one[0].cap == cap;
+}
+
+// Name of a device, looked up once per device: cudaGetDeviceProperties takes
+// milliseconds, and a build between two of its stage events must not wait for it.
+std::string device_name(int device) {
+    static std::mutex mu;
+    static std::vector<std::pair<int, std::string>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const auto &e : cache)
+        if (e.first == device) return e.second;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return "";
+    }
+    cache.emplace_back(device, prop.name);
+    return prop.name;
+}
+
+// Size classes of the ladder: partition counts.
+constexpr uint32_t kClasses[] = {16, 64, 256, 1024, 2048, 4096};
+
+}  // namespace
+
+uint32_t choose_search_group(const Worker &w, const phobic_params *params, uint32_t partitions) {
+    if (w.search_group) return w.search_group;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (!g_tune_loaded) {
+        g_tune = parse_table(default_table_path());
+        g_tune_loaded = true;
+    }
+    if (g_tune.empty()) return 0;
+    const std::string dev = device_name(w.device);
+    uint32_t cap = 0, kmax = 0;
+    if (check_params(params, &cap, &kmax, nullptr) != PHOBIC_OK) return 0;
+    const TuneLine *best = nullptr;
+    for (const auto &t : g_tune)
+        if (t.device == dev && t.P == params->partition_size && t.B == params->buckets && t.cap == cap &&
+            t.max_parts >= partitions && (!best || t.max_parts < best->max_parts))
+            best = &t;
+    return best ? best->group : 0;
+}
+
+phobic_status autotune(Worker &w, const phobic_params *params, const char *path, uint32_t *lines_written,
+                       std::string *err) {
+    uint32_t cap = 0, kmax = 0;
+    phobic_status st = check_params(params, &cap, &kmax, err);
+    if (st != PHOBIC_OK) return st;
+    PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
+    const std::string dev = device_name(w.device);
+    const uint32_t P = params->partition_size, B = params->buckets;
+    const uint64_t max_keys = (uint64_t)kClasses[sizeof(kClasses) / sizeof(kClasses[0]) - 1] * P;
+    uint64_t *keys = nullptr;
+    uint32_t *pil = nullptr, *off = nullptr;
+    const uint64_t max_parts = (max_keys + P - 1) / P;
+    auto cleanup = [&] {
+        if (keys) cudaFree(keys);
+        if (pil) cudaFree(pil);
+        if (off) cudaFree(off);
+        cudaGetLastError();
+    };
+    if (cudaMalloc(&keys, 8 * max_keys) != cudaSuccess || cudaMalloc(&pil, 4 * (size_t)B * max_parts) != cudaSuccess ||
+        cudaMalloc(&off, 4 * (max_parts + 1)) != cudaSuccess) {
+        cleanup();
+        if (err) *err = "autotune: no device memory for the synthetic keys";
+        return PHOBIC_ERR_OOM;
+    }
+    const uint32_t saved = w.search_group;
+    std::vector<TuneLine> found;
+    std::vector<std::string> rows;
+    const uint32_t shapes[] = {1, 2, 4};
+    for (uint32_t ci = 0; ci < sizeof(kClasses) / sizeof(kClasses[0]) && st == PHOBIC_OK; ci++) {
+        const uint32_t parts = kClasses[ci];
+        const uint64_t n = (uint64_t)parts * P;
+        if (launch_splitmix(keys, n, 0x7475ull + ci, w.stream) != cudaSuccess) {
+            st = cuda_status(cudaGetLastError(), "autotune keys", err);
+            break;
+        }
+        phobic_keys k{PHOBIC_KEYS_U64, 1, n, keys, nullptr};
+        phobic_result r{1, pil, off};
+        double ms[3] = {0, 0, 0};
+        for (int si = 0; si < 3 && st == PHOBIC_OK; si++) {
+            w.search_group = shapes[si];
+            double best = 1e30;
+            for (int rep = 0; rep < 4 && st == PHOBIC_OK; rep++) {  // one warm-up, best of three
+                phobic_timings t{};
+                st = enqueue_sets(w, &k, 1, params, &r, nullptr, err);
+                if (st == PHOBIC_OK) st = finish_sets(w, nullptr, &t, err);
+                if (rep > 0 && t.total < best) best = t.total;
+            }
+            ms[si] = best;
+        }
+        if (st != PHOBIC_OK) break;
+        const int win = (int)(std::min_element(ms, ms + 3) - ms);
+        found.push_back(TuneLine{dev, P, B, cap, parts, shapes[win]});
+        char row[512];
+        std::snprintf(row, sizeof(row), "%s\t%u\t%u\t%u\t%u\t%u\t%.4f\t%.4f\t%.4f", dev.c_str(), P, B, cap, parts,
+                      shapes[win], ms[0], ms[1], ms[2]);
+        rows.push_back(row);
+    }
+    w.search_group = saved;
+    cleanup();
+    if (st != PHOBIC_OK) return st;
+    const std::string out_path = path && *path ? std::string(path) : default_table_path();
+    // Keep the other lines of the table (other devices and parameters), replace ours.
+    std::vector<std::string> keep;
+    {
+        std::ifstream f(out_path);
+        std::string line;
+        while (std::getline(f, line)) {
+            if (line.empty() || line[0] == '#') continue;
+            auto parsed = parse_table_line_matches(line, dev, P, B, cap);
+            if (!parsed) keep.push_back(line);
+        }
+    }
+    std::ofstream o(out_path, std::ios::trunc);
+    if (!o) {
+        if (err) *err = "autotune: cannot write " + out_path;
+        return PHOBIC_ERR_INVALID;
+    }
+    o << "# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group"
+         "\tbuild_ms_group1\tbuild_ms_group2\tbuild_ms_group4\n";
+    for (const auto &l : keep) o << l << "\n";
+    for (const auto &l : rows) o << l << "\n";
+    o.close();
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune = parse_table(out_path);
+        g_tune_loaded = true;
+    }
+    if (lines_written) *lines_written = (uint32_t)rows.size();
+    return PHOBIC_OK;
+}
+
+}  // namespace phobicb200

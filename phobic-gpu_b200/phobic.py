@@ -74,6 +74,10 @@ class Timings(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class Tuning(C.Structure):
+    _fields_ = [("search_group", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [
         ("device", C.c_int32),
@@ -152,6 +156,8 @@ def _lib() -> C.CDLL:
         "phobic_debug_change_key": (I32, [U64, U64]),
         "phobic_measure_int_peak": (I32, [P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
         "phobic_ctx_kernel_arch": (I32, [P, C.POINTER(I32)]),
+        "phobic_ctx_set_tuning": (I32, [P, C.POINTER(Tuning)]),
+        "phobic_autotune": (I32, [P, C.POINTER(Params), C.c_char_p, C.POINTER(U32)]),
         "phobic_server_create": (I32, [C.POINTER(ServerConfig), PP]),
         "phobic_server_submit": (I32, [P, C.POINTER(Keys), C.POINTER(Params), C.POINTER(Result), C.POINTER(U64)]),
         "phobic_server_poll": (I32, [P, U64, C.POINTER(I32), C.POINTER(I32)]),
@@ -381,6 +387,20 @@ class Context:
         st = C.c_int()
         check(_lib().phobic_debug_stalled_wait(self.handle, wait_ms, C.byref(st)), self)
         return int(st.value)
+
+    def set_tuning(self, search_group: int = 0) -> None:
+        """Launch shapes of later builds: warps per partition of the search (0 = automatic)."""
+        t = Tuning()
+        t.search_group = search_group
+        check(_lib().phobic_ctx_set_tuning(self.handle, C.byref(t)), self)
+
+    def autotune(self, cfg: "MPHFconfig", path: str | None = None) -> int:
+        """Time the search shapes for a ladder of sizes at cfg's parameters and write the
+        fastest per size class to the tuning table (phobic_autotune); returns lines written."""
+        n = C.c_uint32()
+        check(_lib().phobic_autotune(self.handle, C.byref(cfg.params), path.encode() if path else None,
+                                     C.byref(n)), self)
+        return int(n.value)
 
     def int_peak(self) -> tuple[float, float]:
         """(32-bit integer ops per second, kernel ms) of the pilot hash's mixing round on this

@@ -47,14 +47,61 @@ def main() -> int:
         got = ctx.build((data, offs), cfg)
         want = O.build(O.hash_keys((data, offs), "strings"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs())
         assert np.array_equal(got.pilots, want["pilots"])
+        for group in (1, 2, 4):  # every search shape, on the same keys
+            ctx.set_tuning(search_group=group)
+            for lam, P, n in ((5.0, 2048, 1_000_000), (8.0, 8192, 200_000), (7.5, 4096, 300_000), (3.0, 64, 5000)):
+                g_cfg = phobic.MPHFconfig(lam, P)
+                keys = keygen.splitmix64(700 + n % 1000, n)
+                w = O.build(O.hash_keys(keys, "u64"), P, g_cfg.bucketCountPerPartition, g_cfg.getFulcs())
+                if w["status"] != 0:  # the same error status as the oracle
+                    try:
+                        ctx.build(keys, g_cfg)
+                        raise AssertionError(f"no error for {(group, lam, P, n)}")
+                    except phobic.PhobicError as e:
+                        assert e.status == w["status"], (group, lam, P, n, e.status)
+                    continue
+                got = ctx.build(keys, g_cfg)
+                assert np.array_equal(got.pilots, w["pilots"]), (group, lam, P, n)
+        ctx.set_tuning(search_group=0)
         sets = [keygen.splitmix64(200 + i, 1000 * (i + 1)) for i in range(12)]
         res, st = phobic.build_batch(ctx, sets, cfg)
         for ks, r in zip(sets, res):
             w = O.build(O.hash_keys(ks, "u64"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs())
             assert np.array_equal(r.pilots, w["pilots"])
-        compiled, lines = ctx.checks()
+        compiled, lines = ctx.checks(reset=True)
         print("checked builds:", len(cases) + 2, "failed check lines (map, partition, search):", lines)
-        return 0 if lines == [0, 0, 0] else 1
+        if lines != [0, 0, 0]:
+            return 1
+        # Keys that change between the passes (injected from the host), on the regular and
+        # the no-allocation build: the status must say so.  The clamps that keep such a
+        # build's stores inside its arrays fire here by design; the first fired check of
+        # each kernel file is printed for the record.
+        import ctypes as C
+
+        import torch
+
+        cfg = phobic.MPHFconfig(7.0, 2500)
+        keys = keygen.splitmix64(62, 500_000)
+        dk = torch.from_numpy(keys.view(np.int64)).cuda()
+        phobic.debug_change_key(499_999, 0xFFFF_0000_0000_0000)
+        try:
+            ctx.build(dk, cfg)
+            raise AssertionError("keys changed, yet the build succeeded")
+        except phobic.PhobicError as e:
+            assert e.status == phobic.ERR_KEYS_CHANGED, e.status
+        dk.copy_(torch.from_numpy(keys.view(np.int64)))
+        parts = cfg.partitions(len(keys))
+        dp = torch.zeros(parts * cfg.bucketCountPerPartition, dtype=torch.int32, device="cuda")
+        do = torch.zeros(parts + 1, dtype=torch.int32, device="cuda")
+        k = phobic.Keys(phobic.KEYS_U64, 1, len(keys), dk.data_ptr(), None)
+        r = phobic.Result(1, dp.data_ptr(), do.data_ptr())
+        torch.cuda.synchronize()
+        phobic.debug_change_key(12_345, 0x5A5A_0000_FFFF_0001)
+        st = phobic.lib().phobic_build_noalloc(C.byref(k), C.byref(cfg.params), C.byref(r), None)
+        assert st == phobic.ERR_KEYS_CHANGED, st
+        _, fired = ctx.checks(reset=True)
+        print("keys-changed builds: status ok; first clamp fired (map, partition, search):", fired)
+        return 0
 
 
 if __name__ == "__main__":
