@@ -317,14 +317,31 @@ __global__ void __launch_bounds__(kChunkThreads, 1) k_chunk_str(MapArgs a) {
     const uint64_t hi = lo + a.chunk < a.total_keys ? lo + a.chunk : a.total_keys;
     SetCache sc;
     uint32_t bad_set = 0xFFFFFFFFu;
-    for (uint64_t gbase = lo + 32 * (uint64_t)warp; gbase < hi; gbase += 32 * (uint64_t)(kChunkThreads / 32)) {
+    constexpr uint64_t kGroupStride = 32 * (uint64_t)(kChunkThreads / 32);
+    // The next group's offsets are loaded while the current group is staged and hashed
+    // (when they lie in the set of the current lane's key), so a group waits for one
+    // round trip to memory (its bytes), not two (offsets, then bytes).
+    bool have_next = false;
+    uint64_t a_next = 0, b_next = 0;
+    for (uint64_t gbase = lo + 32 * (uint64_t)warp; gbase < hi; gbase += kGroupStride) {
         const uint64_t g = gbase + lane;
         const bool valid = g < hi;
         uint64_t a_off = 0, b_off = 0;
         if (valid) {
-            sc.locate(a, g);
-            a_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo));
-            b_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo) + 1);
+            if (have_next) {
+                a_off = a_next;
+                b_off = b_next;
+            } else {
+                sc.locate(a, g);
+                a_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo));
+                b_off = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (g - sc.lo) + 1);
+            }
+        }
+        const uint64_t gn = g + kGroupStride;
+        have_next = valid && gn < hi && gn < sc.hi;  // same set as this lane's key: sc stays valid
+        if (have_next) {
+            a_next = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (gn - sc.lo));
+            b_next = __ldg(reinterpret_cast<const unsigned long long *>(sc.offsets) + (gn - sc.lo) + 1);
         }
         const uint32_t vmask = __ballot_sync(kFullMask, valid);
         const int last = 31 - __clz(vmask);
