@@ -295,6 +295,19 @@ __device__ __noinline__ bool has_duplicate_key(uint2 L, uint32_t s, int lane) {
     return __any_sync(kFullMask, d);
 }
 
+// Marks slot q (and its mirror q + ps) when `on`; predicated shared-memory reductions, so
+// the lanes of a bucket mark without a divergent branch.
+__device__ __forceinline__ void mark_if(uint32_t *occ, uint32_t q, uint32_t ps, bool on) {
+    const uint32_t m = q + ps;
+    const uint32_t a0 = (uint32_t)__cvta_generic_to_shared(occ + (q >> 5)), a1 =
+                           (uint32_t)__cvta_generic_to_shared(occ + (m >> 5));
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %4, 0;\n\t"
+        "@p red.shared.or.b32 [%0], %1;\n\t@p red.shared.or.b32 [%2], %3;\n\t}" ::"r"(a0),
+        "r"(1u << (q & 31)), "r"(a1), "r"(1u << (m & 31)), "r"((uint32_t)on)
+        : "memory");
+}
+
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
 __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
                                                 uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
@@ -302,7 +315,10 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
     const uint32_t padded = (s + 3) & ~3u;
     for (uint32_t k = 0; k < k_lim; k++) {
         if (k == kDupCheckAt && s > 1 && has_duplicate_key(L, s, lane)) return PHOBIC_ERR_DUPLICATE_KEY;
-        const uint32_t h = mine ? fm.mod(pilot_hash(L.x, L.y, k)) : (0x80000000u | lane);
+        // Every lane hashes (no divergent branch); lanes past the bucket take distinct
+        // out-of-range values, so they never collide.
+        const uint32_t hk = fm.mod(pilot_hash(L.x, L.y, k));
+        const uint32_t h = mine ? hk : (0x80000000u | lane);
         if (s > 1) {
             uint32_t m = __match_any_sync(kFullMask, h);
             if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
@@ -323,11 +339,9 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
             __syncwarp();
         }
         if (o == kNone) continue;
-        if (mine) {
-            uint32_t q = h + o;
-            q = q >= ps ? q - ps : q;
-            if (PHB_CHECK(q < ps)) mark(ws.occ, q, ps);
-        }
+        uint32_t q = hk + o;
+        q = q >= ps ? q - ps : q;
+        mark_if(ws.occ, q, ps, mine && PHB_CHECK(!mine || q < ps));
         __syncwarp();
         *pilot = o + ps * k;
         return PHOBIC_OK;
