@@ -572,6 +572,70 @@ def build_batch(ctx: Context, key_sets: list, cfg: MPHFconfig, kind: int | None 
     return outs, [int(s) for s in st]
 
 
+# numpy images of phobic_keys and phobic_result (one row per set), for batches of many sets.
+_KEYS_DT = np.dtype({"names": ["kind", "on_device", "n", "data", "offsets"],
+                     "formats": [np.int32, np.int32, np.uint64, np.uint64, np.uint64],
+                     "offsets": [0, 4, 8, 16, 24], "itemsize": 32})
+_RESULT_DT = np.dtype({"names": ["on_device", "pilots", "partition_offsets"],
+                       "formats": [np.int32, np.uint64, np.uint64], "offsets": [0, 8, 16], "itemsize": 24})
+
+
+def batch_layout(sizes, cfg: MPHFconfig) -> tuple[np.ndarray, np.ndarray]:
+    """Start of every set's pilots and partition offsets in flat result arrays (one more
+    entry than sets: the totals), for build_batch_flat."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    parts = (sizes + cfg.partitionSize - 1) // cfg.partitionSize
+    pstart = np.zeros(len(sizes) + 1, np.int64)
+    np.cumsum(parts * cfg.bucketCountPerPartition, out=pstart[1:])
+    ostart = np.zeros(len(sizes) + 1, np.int64)
+    np.cumsum(parts + 1, out=ostart[1:])
+    return pstart, ostart
+
+
+def build_batch_flat(ctx: Context, keys, sizes, cfg: MPHFconfig, pilots=None, offsets=None,
+                     kind: int = KEYS_U64) -> tuple[object, object, np.ndarray, dict]:
+    """Batched build of consecutive sets of one flat key array: set i is the next sizes[i]
+    keys (u64, or 16-byte records with kind BYTES16 / PREHASHED).  Results go to flat arrays
+    (created like the keys when None): set i's pilots start at batch_layout(...)[0][i] and its
+    partition offsets at batch_layout(...)[1][i].  The C structs of all sets are built as
+    numpy arrays, so the host cost does not grow with a Python call per set.  Returns
+    (pilots, offsets, statuses, timings)."""
+    sizes = np.asarray(sizes, dtype=np.int64)
+    nsets = len(sizes)
+    pstart, ostart = batch_layout(sizes, cfg)
+    width = 8 if kind == KEYS_U64 else 16
+    on_dev = _is_cuda(keys)
+    if pilots is None or offsets is None:
+        if on_dev:
+            import torch
+            pilots = torch.empty(max(int(pstart[-1]), 1), dtype=torch.int32, device=keys.device)
+            offsets = torch.empty(int(ostart[-1]), dtype=torch.int32, device=keys.device)
+        else:
+            pilots = np.zeros(max(int(pstart[-1]), 1), np.uint32)
+            offsets = np.zeros(int(ostart[-1]), np.uint32)
+    kstart = np.zeros(nsets, np.int64)
+    if nsets > 1:
+        np.cumsum(sizes[:-1], out=kstart[1:])
+    karr = np.zeros(nsets, _KEYS_DT)
+    karr["kind"] = kind
+    karr["on_device"] = int(on_dev)
+    karr["n"] = sizes
+    karr["data"] = np.uint64(_ptr(keys) or 0) + (kstart * width).astype(np.uint64)
+    rarr = np.zeros(nsets, _RESULT_DT)
+    rarr["on_device"] = int(_is_cuda(pilots))
+    rarr["pilots"] = np.uint64(_ptr(pilots) or 0) + (pstart[:-1] * 4).astype(np.uint64)
+    rarr["partition_offsets"] = np.uint64(_ptr(offsets)) + (ostart[:-1] * 4).astype(np.uint64)
+    st = np.zeros(nsets, np.int32)
+    _torch_first(ctx, keys, pilots, offsets)
+    t = Timings()
+    rc = _lib().phobic_build_batch(ctx.handle, C.cast(karr.ctypes.data, C.POINTER(Keys)), nsets,
+                                   C.byref(cfg.params), C.cast(rarr.ctypes.data, C.POINTER(Result)),
+                                   C.cast(st.ctypes.data, C.POINTER(C.c_int)), C.byref(t))
+    if rc != OK and (st == OK).all():
+        check(rc, ctx)
+    return pilots, offsets, st, t.as_dict()
+
+
 class Server:
     """phobic_server: continuous-batching build server on one device."""
 

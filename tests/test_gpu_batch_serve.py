@@ -30,6 +30,31 @@ def test_batch_equals_plain_builds(phobic, ctx):
             assert ctx.verify(keys, cfg, got) == 0
 
 
+def test_flat_batch_equals_list_batch(phobic, ctx):
+    """build_batch_flat (one key buffer, set sizes, flat results; device and host keys)
+    gives every set the result of build_batch and of the oracle."""
+    torch = pytest.importorskip("torch")
+    cfg = phobic.MPHFconfig(6.0, 2048)
+    sizes = np.array([0, 1, 5, 2047, 2048, 2049, 10_000, 0, 77_777, 3])
+    keys = keygen.splitmix64(900, int(sizes.sum()))
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    sets = [keys[starts[i]:starts[i + 1]] for i in range(len(sizes))]
+    outs, st = phobic.build_batch(ctx, sets, cfg)
+    assert st == [0] * len(sets)
+    pstart, ostart = phobic.batch_layout(sizes, cfg)
+    for flat_keys in (torch.from_numpy(keys.view(np.int64)).cuda(), keys):
+        fp, fo, fst, _ = phobic.build_batch_flat(ctx, flat_keys, sizes, cfg)
+        assert (fst == 0).all()
+        fp = fp.cpu().numpy().view(np.uint32) if hasattr(fp, "cpu") else fp
+        fo = fo.cpu().numpy().view(np.uint32) if hasattr(fo, "cpu") else fo
+        for i, got in enumerate(outs):
+            assert (fp[pstart[i]:pstart[i + 1]] == got.pilots).all(), i
+            assert (fo[ostart[i]:ostart[i + 1]] == got.partition_offsets).all(), i
+    for i in (2, 5, 8):
+        want = oracle(O.hash_keys(sets[i], "u64"), cfg)
+        assert (outs[i].pilots == want["pilots"]).all()
+
+
 def test_batch_many_small_sets_log_uniform(phobic, ctx):
     cfg = phobic.MPHFconfig(6.0, 2048)
     sizes = keygen.set_sizes(4, 300, 1000, 200_000)
