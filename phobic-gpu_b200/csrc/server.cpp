@@ -77,14 +77,30 @@ struct phobic_server {
     int running = 0;
     Clock::time_point busy_since;
     uint32_t max_batch = 0, max_running = 0;
-    // Device time of each finished batch, in ms after t0_ev: its first event to its last.
+    // Device time of recent finished batches, in ms after t0_ev (first event to last).  Only
+    // batches close in time can overlap, so the record keeps the latest kSpanWindow spans
+    // and folds the overlap of older ones into max_overlap_seen.
     cudaEvent_t t0_ev = nullptr;
     std::vector<std::pair<float, float>> device_spans;
+    uint32_t max_overlap_seen = 0;
 };
 
 namespace {
 
 constexpr uint64_t kBatchKeyLimit = 0xF0000000ull;  // keys per batch stay below 2^32
+constexpr size_t kSpanWindow = 4096;               // device spans kept for the overlap statistic
+
+// Largest number of spans covering one instant (a span ending at t does not overlap one
+// beginning at t).
+uint32_t max_overlap(const std::vector<std::pair<float, float>> &spans) {
+    std::vector<std::pair<float, int>> ev;
+    ev.reserve(2 * spans.size());
+    for (const auto &sp : spans) ev.emplace_back(sp.first, 1), ev.emplace_back(sp.second, -1);
+    std::sort(ev.begin(), ev.end());
+    int cur = 0, best = 0;
+    for (const auto &e : ev) best = std::max(best, cur += e.second);
+    return (uint32_t)best;
+}
 
 uint64_t held_bytes(const phobic_server *s) {
     uint64_t t = 0;
@@ -122,7 +138,13 @@ void worker_loop(phobic_server *s, StreamWorker *sw) {
         if (!timed) cudaGetLastError();
 
         lk.lock();
-        if (timed) s->device_spans.emplace_back(t_begin, t_end);
+        if (timed) {
+            s->device_spans.emplace_back(t_begin, t_end);
+            if (s->device_spans.size() > kSpanWindow) {
+                s->max_overlap_seen = std::max(s->max_overlap_seen, max_overlap(s->device_spans));
+                s->device_spans.erase(s->device_spans.begin(), s->device_spans.begin() + kSpanWindow / 2);
+            }
+        }
         s->max_batch = std::max<uint32_t>(s->max_batch, (uint32_t)batch.size());
         for (size_t i = 0; i < batch.size(); i++) {
             double ms = std::chrono::duration<double, std::milli>(now - batch[i].submitted).count();
@@ -387,17 +409,7 @@ phobic_status phobic_server_stats_get(phobic_server *s, phobic_server_stats *out
     out->peak_bytes = s->peak_bytes;
     out->max_batch_requests = s->max_batch;
     out->max_batches_in_flight = s->max_running;
-    {
-        // Largest number of device spans covering one instant (a span ending at t does not
-        // overlap one beginning at t).
-        std::vector<std::pair<float, int>> ev;
-        ev.reserve(2 * s->device_spans.size());
-        for (const auto &sp : s->device_spans) ev.emplace_back(sp.first, 1), ev.emplace_back(sp.second, -1);
-        std::sort(ev.begin(), ev.end());
-        int cur = 0, best = 0;
-        for (const auto &e : ev) best = std::max(best, cur += e.second);
-        out->max_device_overlap = (uint32_t)best;
-    }
+    out->max_device_overlap = std::max(s->max_overlap_seen, max_overlap(s->device_spans));
     if (!s->latencies.empty()) {
         std::vector<double> l = s->latencies;
         std::sort(l.begin(), l.end());

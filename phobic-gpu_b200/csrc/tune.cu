@@ -211,9 +211,11 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
             if (!parsed) keep.push_back(line);
         }
     }
-    std::ofstream o(out_path, std::ios::trunc);
+    // Written beside the table and renamed over it, so a reader never sees half a table.
+    const std::string tmp_path = out_path + ".tmp";
+    std::ofstream o(tmp_path, std::ios::trunc);
     if (!o) {
-        if (err) *err = "autotune: cannot write " + out_path;
+        if (err) *err = "autotune: cannot write " + tmp_path;
         return PHOBIC_ERR_INVALID;
     }
     o << "# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group"
@@ -221,6 +223,11 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
     for (const auto &l : keep) o << l << "\n";
     for (const auto &l : rows) o << l << "\n";
     o.close();
+    if (!o || std::rename(tmp_path.c_str(), out_path.c_str()) != 0) {
+        std::remove(tmp_path.c_str());
+        if (err) *err = "autotune: cannot replace " + out_path;
+        return PHOBIC_ERR_INVALID;
+    }
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         g_tune = parse_table(out_path);

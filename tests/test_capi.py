@@ -107,3 +107,29 @@ def test_context_without_device_fails_loudly(phobic):
     with pytest.raises(phobic.PhobicError) as e:
         phobic.Context(0)
     assert e.value.status == phobic.ERR_NO_DEVICE
+
+
+def test_shipped_tuning_table_is_well_formed(phobic):
+    """phobic-gpu_b200/tuning.tsv (written by phobic_autotune on a B200): tab-separated lines
+    of device, P, B, partition capacity, size class, search shape and the three measured
+    build times; for every parameter set the classes ascend and the chosen shape is the
+    fastest measured one."""
+    table = ROOT / "phobic-gpu_b200" / "tuning.tsv"
+    rows = [l.split("\t") for l in table.read_text().splitlines() if l and not l.startswith("#")]
+    assert rows
+    groups = {}
+    for r in rows:
+        assert len(r) == 9, r
+        dev, P, B, cap, cls, shape = r[0], *map(int, r[1:6])
+        ms = [float(x) for x in r[6:9]]
+        assert shape in (1, 2, 4)
+        assert ms[[1, 2, 4].index(shape)] == min(ms), r
+        cfg = None
+        for lam in (4.5, 5.0, 6.0, 7.0, 7.5):
+            c = phobic.MPHFconfig(lam, P)
+            if c.bucketCountPerPartition == B:
+                cfg = c
+        assert cfg is not None and cfg.params.max_partition_size == cap, r
+        groups.setdefault((dev, P, B, cap), []).append(cls)
+    for key, classes in groups.items():
+        assert classes == sorted(classes) and len(set(classes)) == len(classes), key
