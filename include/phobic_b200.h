@@ -121,9 +121,10 @@ PHOBIC_API phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tun
 
 /* No counterpart in the reference (its shapes are per-pipeline specialisation constants,
  * src/search_stage.cpp:36-37).  Autotuner: builds synthetic u64 keys (splitmix64 on the
- * device) of 16, 64, 256, 1024, 2048 and 4096 partitions at these parameters with every
- * search shape (phobic_tuning::search_group 1, 2, 4), and writes the fastest shape per
- * size class, with the measured build times, to the tab-separated tuning table at path
+ * device) of 16, 64, 256, 512, 768, 1024, 2048 and 4096 partitions at these parameters with every
+ * search shape (phobic_tuning::search_group 1, 2, 4) on three key sets per size (a small
+ * build lasts as long as its slowest partition, which varies with the keys), and writes the
+ * shape with the lowest mean build time per size class, with those times, to the tab-separated tuning table at path
  * (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv in the package directory beside the
  * library's lib/), keeping the table's lines for other devices and parameters.  Builds
  * with automatic tuning then take their shape from the table: the line of their device,

@@ -199,8 +199,8 @@ cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t s
 // warp per partition, 0 = chosen from the partition count (search_group_for).
 cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, int group = 0);
 // Default group size when the autotuner's table has no line for a build: 4 warps per
-// partition when the partitions fill at most a twelfth of the one-warp kernel's warp
-// slots, 2 up to a quarter, else 1.
+// partition up to 512 partitions, 2 up to 1024, else 1, each only while the groups fit one
+// wave of the group kernel.
 int search_group_for(uint32_t partitions, int sm_count);
 size_t search_group_smem(uint32_t buckets, uint32_t cap, int W);
 // First failed bounds check of each kernel file in the checked build (source line, 0 =

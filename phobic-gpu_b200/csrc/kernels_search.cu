@@ -906,12 +906,14 @@ static cudaError_t launch_group(const SearchArgs &a, int sm_count, cudaStream_t 
 }
 
 int search_group_for(uint32_t partitions, int sm_count) {
-    // Warp slots of the one-warp kernel: kSearchWarps * kSearchCtasPerSm per SM (4736 on a
-    // B200).  Measured on a B200 (the autotuner's ladder at six parameter sets): groups of 4
-    // are fastest up to about 256 partitions, groups of 2 around 1024, one warp from 2048 on.
-    const uint64_t slots = (uint64_t)(sm_count > 0 ? sm_count : 148) * kSearchWarps * kSearchCtasPerSm;
-    if ((uint64_t)partitions * 12 <= slots) return 4;
-    if ((uint64_t)partitions * 4 <= slots) return 2;
+    // Measured on a B200 (the autotuner's ladder, three key sets per size): groups of 4 are
+    // fastest up to about 256 partitions and protect against retry-heavy partitions (a small
+    // build lasts as long as its slowest one), groups of 2 around 1024, one warp beyond.  A
+    // group must fit one wave of the group kernel (2 CTAs of kSearchWarps warps per SM).
+    const uint64_t sms = (uint64_t)(sm_count > 0 ? sm_count : 148);
+    const uint64_t wave = sms * 2 * kSearchWarps;  // warps of one wave of the group kernel
+    if ((uint64_t)partitions * 4 <= wave && partitions <= 512) return 4;
+    if ((uint64_t)partitions * 2 <= wave && partitions <= 1024) return 2;
     return 1;
 }
 

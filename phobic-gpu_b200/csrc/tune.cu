@@ -8,8 +8,9 @@
 // groups of 2 or 4 when a build has few partitions and each partition's search is
 // bound by the latency of its sequential tries.
 //
-// phobic_autotune times every shape on synthetic keys (splitmix64 on the device) for a
-// ladder of partition counts at the caller's parameters, and records the fastest
+// phobic_autotune times every shape on synthetic keys (splitmix64 on the device; three key
+// sets per size, the mean of their best-of-three build times) for a ladder of partition
+// counts at the caller's parameters, and records the fastest
 // per (device name, P, B, partition capacity, size class) as one line of a tab-
 // separated table:
 //     device  partition_size  buckets  max_partition_size  max_partitions  search_group  [ms per shape...]
@@ -116,7 +117,8 @@ std::string device_name(int device) {
 }
 
 // Size classes of the ladder: partition counts.
-constexpr uint32_t kClasses[] = {16, 64, 256, 1024, 2048, 4096};
+constexpr uint32_t kClasses[] = {16, 64, 256, 512, 768, 1024, 2048, 4096};
+constexpr uint32_t kTuneKeySets = 3;  // key sets timed per class and shape
 
 }  // namespace
 
@@ -170,23 +172,27 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
     for (uint32_t ci = 0; ci < sizeof(kClasses) / sizeof(kClasses[0]) && st == PHOBIC_OK; ci++) {
         const uint32_t parts = kClasses[ci];
         const uint64_t n = (uint64_t)parts * P;
-        if (launch_splitmix(keys, n, 0x7475ull + ci, w.stream) != cudaSuccess) {
-            st = cuda_status(cudaGetLastError(), "autotune keys", err);
-            break;
-        }
         phobic_keys k{PHOBIC_KEYS_U64, 1, n, keys, nullptr};
         phobic_result r{1, pil, off};
+        // A small build lasts as long as its slowest partition, which varies with the keys:
+        // each shape is timed on kTuneKeySets key sets and scored by the sum of their times.
         double ms[3] = {0, 0, 0};
-        for (int si = 0; si < 3 && st == PHOBIC_OK; si++) {
-            w.search_group = shapes[si];
-            double best = 1e30;
-            for (int rep = 0; rep < 4 && st == PHOBIC_OK; rep++) {  // one warm-up, best of three
-                phobic_timings t{};
-                st = enqueue_sets(w, &k, 1, params, &r, nullptr, err);
-                if (st == PHOBIC_OK) st = finish_sets(w, nullptr, &t, err);
-                if (rep > 0 && t.total < best) best = t.total;
+        for (uint32_t ks = 0; ks < kTuneKeySets && st == PHOBIC_OK; ks++) {
+            if (launch_splitmix(keys, n, 0x7475ull + 97 * ci + 7919 * ks, w.stream) != cudaSuccess) {
+                st = cuda_status(cudaGetLastError(), "autotune keys", err);
+                break;
             }
-            ms[si] = best;
+            for (int si = 0; si < 3 && st == PHOBIC_OK; si++) {
+                w.search_group = shapes[si];
+                double best = 1e30;
+                for (int rep = 0; rep < 4 && st == PHOBIC_OK; rep++) {  // one warm-up, best of three
+                    phobic_timings t{};
+                    st = enqueue_sets(w, &k, 1, params, &r, nullptr, err);
+                    if (st == PHOBIC_OK) st = finish_sets(w, nullptr, &t, err);
+                    if (rep > 0 && t.total < best) best = t.total;
+                }
+                ms[si] += best / kTuneKeySets;
+            }
         }
         if (st != PHOBIC_OK) break;
         const int win = (int)(std::min_element(ms, ms + 3) - ms);

@@ -1,9 +1,9 @@
 """Sweep of the search's launch shapes (warps per partition) across workload sizes.
 
-    python phobic-gpu_b200/shape_sweep.py [--device 0]
+    python phobic-gpu_b200/shape_sweep.py [--device 0] [--seeds 11] [--cases C1,C2,...]
 
-For each case (the parameter sets and set sizes of the benchmark workloads), builds the
-same synthetic u64 keys (splitmix64 on the device, seed 11) with every shape of the
+For each case (the parameter sets and set sizes of the benchmark workloads) and seed,
+builds the same synthetic u64 keys (splitmix64 on the device) with every shape of the
 search (phobic_tuning::search_group 1, 2, 4, and 0 = automatic), device-resident keys
 and results, and prints one JSON line per case: build and search ms per shape (CUDA
 events on the context's stream) and whether each shape's pilots equal the one-warp
@@ -34,17 +34,23 @@ def main() -> None:
 
     ap = argparse.ArgumentParser()
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--seeds", default="11", help="comma-separated key seeds")
+    ap.add_argument("--cases", default="", help="comma-separated case names (default: all)")
     args = ap.parse_args()
+    seeds = [int(x) for x in args.seeds.split(",")]
+    wanted = {c for c in args.cases.split(",") if c}
     torch.cuda.set_device(args.device)
     ctx = phobic.Context(args.device)
     stream = torch.cuda.ExternalStream(ctx.stream_handle())
-    for name, lam, P, n in CASES:
+    for (name, lam, P, n), seed in [(c, sd) for c in CASES for sd in seeds]:
+        if wanted and name not in wanted:
+            continue
         cfg = phobic.MPHFconfig(lam, P)
-        keys = keygen.splitmix64_cuda(11, n)
+        keys = keygen.splitmix64_cuda(seed, n)
         parts, B = cfg.partitions(n), cfg.bucketCountPerPartition
         dp = torch.empty(max(parts * B, 1), dtype=torch.int32, device="cuda")
         do = torch.empty(parts + 1, dtype=torch.int32, device="cuda")
-        row = {"case": name, "lambda": lam, "P": P, "n": n, "partitions": parts}
+        row = {"case": name, "seed": seed, "lambda": lam, "P": P, "n": n, "partitions": parts}
         ref = None
         for g in (1, 2, 4, 0):
             ctx.set_tuning(search_group=g)

@@ -94,11 +94,11 @@ def test_autotune_writes_its_table_and_builds_still_match(phobic, tmp_path):
     table.write_text("# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group\n"
                      "Some Other GPU\t2048\t410\t3072\t64\t2\n")
     with phobic.Context(0) as ctx:
-        assert ctx.autotune(cfg, str(table)) == 6
+        assert ctx.autotune(cfg, str(table)) == 8
         lines = [l.split("\t") for l in table.read_text().splitlines() if l and not l.startswith("#")]
         assert ["Some Other GPU", "2048", "410", "3072", "64", "2"] in [l[:6] for l in lines]
         ours = [l for l in lines if l[0] != "Some Other GPU"]
-        assert [int(l[4]) for l in ours] == [16, 64, 256, 1024, 2048, 4096]
+        assert [int(l[4]) for l in ours] == [16, 64, 256, 512, 768, 1024, 2048, 4096]
         assert all(l[5] in ("1", "2", "4") and len(l) == 9 for l in ours)
         keys = keygen.splitmix64(9, 1_000_000)
         got = ctx.build(keys, cfg)
