@@ -115,3 +115,74 @@ def test_noalloc_rejects_builds_larger_than_its_scratch(phobic):
     k = phobic.Keys(phobic.KEYS_U64, 1, n, dk.data_ptr(), None)
     r = phobic.Result(1, dp.data_ptr(), do.data_ptr())
     assert fn(C.byref(k), C.byref(cfg.params), C.byref(r), None) == phobic.ERR_BUDGET
+
+
+def test_noalloc_timeout_then_busy_until_the_work_drains(phobic, monkeypatch):
+    """A call whose work cannot finish within PHOBIC_TIMEOUT_MS returns PHOBIC_ERR_TIMEOUT
+    and leaves its work queued; until that work has run, the static array is in use and
+    another call returns PHOBIC_ERR_BUSY without queueing anything.  Once the stream has
+    drained, calls build correctly again.  The work is held back by a bounded sleep kernel
+    queued ahead of it on the same stream (about 50 ms), not by anything that can hang."""
+    import time
+
+    torch = pytest.importorskip("torch")
+    fn = _fn(phobic)
+    stream = torch.cuda.Stream()
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(36, 100_000)
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    parts = cfg.partitions(len(keys))
+    dp = torch.zeros(parts * cfg.bucketCountPerPartition, dtype=torch.int32, device="cuda")
+    do = torch.zeros(parts + 1, dtype=torch.int32, device="cuda")
+    k = phobic.Keys(phobic.KEYS_U64, 1, len(keys), dk.data_ptr(), None)
+    r = phobic.Result(1, dp.data_ptr(), do.data_ptr())
+    torch.cuda.synchronize()
+    assert fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream)) == phobic.OK
+    monkeypatch.setenv("PHOBIC_TIMEOUT_MS", "1")
+    with torch.cuda.stream(stream):
+        torch.cuda._sleep(100_000_000)  # ~50 ms of spinning on the build's stream
+    assert fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream)) == phobic.ERR_TIMEOUT
+    assert fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream)) == phobic.ERR_BUSY
+    monkeypatch.delenv("PHOBIC_TIMEOUT_MS")
+    stream.synchronize()
+    status = phobic.ERR_BUSY
+    for _ in range(200):  # the release runs as a host function behind the drained work
+        status = fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream))
+        if status != phobic.ERR_BUSY:
+            break
+        time.sleep(0.01)
+    assert status == phobic.OK
+    with phobic.Context(0) as ctx:
+        want = ctx.build(keys, cfg)
+    assert np.array_equal(dp.cpu().numpy().view(np.uint32), want.pilots)
+    assert np.array_equal(do.cpu().numpy().view(np.uint32), want.partition_offsets)
+
+
+def test_noalloc_refuses_a_capturing_stream(phobic):
+    """The call is synchronous, so it must not be captured into a CUDA graph: on a stream
+    that is capturing it returns PHOBIC_ERR_INVALID and queues nothing (the graph stays
+    empty); the same call outside the capture builds normally."""
+    torch = pytest.importorskip("torch")
+    fn = _fn(phobic)
+    cfg = phobic.MPHFconfig(7.0, 2500)
+    keys = keygen.splitmix64(37, 50_000)
+    dk = torch.from_numpy(keys.view(np.int64)).cuda()
+    parts = cfg.partitions(len(keys))
+    dp = torch.zeros(parts * cfg.bucketCountPerPartition, dtype=torch.int32, device="cuda")
+    do = torch.zeros(parts + 1, dtype=torch.int32, device="cuda")
+    k = phobic.Keys(phobic.KEYS_U64, 1, len(keys), dk.data_ptr(), None)
+    r = phobic.Result(1, dp.data_ptr(), do.data_ptr())
+    torch.cuda.synchronize()
+    import warnings
+
+    stream = torch.cuda.Stream()
+    graph = torch.cuda.CUDAGraph()
+    with warnings.catch_warnings():
+        warnings.filterwarnings("ignore", message="The CUDA Graph is empty")  # nothing was queued, by design
+        with torch.cuda.graph(graph, stream=stream):
+            status = fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream))
+    assert status == phobic.ERR_INVALID
+    assert fn(C.byref(k), C.byref(cfg.params), C.byref(r), C.c_void_p(stream.cuda_stream)) == phobic.OK
+    with phobic.Context(0) as ctx:
+        want = ctx.build(keys, cfg)
+    assert np.array_equal(dp.cpu().numpy().view(np.uint32), want.pilots)
