@@ -105,10 +105,15 @@ typedef struct phobic_timings {
  * specialisation constants fixed per pipeline, src/search_stage.cpp:36-37). */
 typedef struct phobic_tuning {
     /* Warps that search one partition together, each trying its own pilot counter per
-     * step (pilots per probe): 1, 2 or 4; 0 = from the autotuner's table when it holds
+     * step (pilots per probe): 1, 2, 4 or 8; 0 = from the autotuner's table when it holds
      * these parameters, else from the partition count. */
     uint32_t search_group;
-    uint32_t reserved[7];
+    /* With search_group 2, 4 or 8: 1 = the group searches several small buckets at once
+     * (bucket pipeline: warp w takes the w-th next bucket of at most 32 keys, results are
+     * committed in order while their slots stay free), 0 = several pilot counters of one
+     * bucket (k-split).  Either way the pilots are those of the sequential search. */
+    uint32_t search_pipeline;
+    uint32_t reserved[6];
 } phobic_tuning;
 
 typedef struct phobic_ctx phobic_ctx;
@@ -121,15 +126,17 @@ PHOBIC_API phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tun
 
 /* No counterpart in the reference (its shapes are per-pipeline specialisation constants,
  * src/search_stage.cpp:36-37).  Autotuner: builds synthetic u64 keys (splitmix64 on the
- * device) of 16, 64, 256, 512, 768, 1024, 2048 and 4096 partitions at these parameters with every
- * search shape (phobic_tuning::search_group 1, 2, 4) on three key sets per size (a small
- * build lasts as long as its slowest partition, which varies with the keys), and writes the
- * shape with the lowest mean build time per size class, with those times, to the tab-separated tuning table at path
- * (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv in the package directory beside the
- * library's lib/), keeping the table's lines for other devices and parameters.  Builds
- * with automatic tuning then take their shape from the table: the line of their device,
- * partition size, bucket count and partition capacity with the smallest size class that
- * holds their partition count.  *lines_written (optional) = size classes written. */
+ * device) of 16, 64, 256, 512, 768, 1024, 2048 and 4096 partitions at these parameters with
+ * every search shape it knows (one warp per partition; k-split groups of 2 and 4 warps;
+ * bucket pipelines of 2, 4 and 8 warps) on three key sets per size (a build of few
+ * partitions lasts as long as its slowest partition, which varies with the keys), and writes
+ * the shape with the lowest mean build time per size class, with every measured time, to the
+ * tab-separated tuning table at path (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv in the
+ * package directory beside the library's lib/), keeping the table's lines for other devices
+ * and parameters.  Builds with automatic tuning then take their shape from the table: the
+ * line of their device, partition size, bucket count and partition capacity with the smallest
+ * size class that holds their partition count.  *lines_written (optional) = size classes
+ * written. */
 PHOBIC_API phobic_status phobic_autotune(phobic_ctx *ctx, const phobic_params *params, const char *path,
                                          uint32_t *lines_written);
 

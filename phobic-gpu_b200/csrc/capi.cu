@@ -280,9 +280,12 @@ phobic_status phobic_debug_checks(phobic_ctx *ctx, int *compiled, uint32_t *line
 
 phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tuning *t) {
     if (!ctx || !t) return PHOBIC_ERR_INVALID;
-    if (t->search_group != 0 && t->search_group != 1 && t->search_group != 2 && t->search_group != 4)
+    if (t->search_group != 0 && t->search_group != 1 && t->search_group != 2 && t->search_group != 4 &&
+        t->search_group != 8)
         return PHOBIC_ERR_INVALID;
+    if (t->search_pipeline > 1) return PHOBIC_ERR_INVALID;
     ctx->w.search_group = t->search_group;
+    ctx->w.search_pipeline = t->search_pipeline;
     return PHOBIC_OK;
 }
 

@@ -590,7 +590,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
                   k_max, d_queue, d_err, d_pcur};
     {
         StageRange r("search (K4)");
-        PHB_TRY(launch_search(qa, w.sm_count, s, choose_search_group(w, params, (uint32_t)M)), "K4 search");
+        PHB_TRY(launch_search(qa, w.sm_count, s, choose_search_shape(w, params, (uint32_t)M)), "K4 search");
     }
     PHB_TRY(cudaEventRecord(w.ev[5], s), "event");
 

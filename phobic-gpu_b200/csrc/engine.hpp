@@ -12,6 +12,8 @@
 
 namespace phobicb200 {
 
+struct SearchShape;
+
 // A grow-only device memory pool carved into 256-byte aligned slices; every
 // slice lives until the next reset().  One arena serves one stream, so reuse
 // across builds is ordered by that stream.
@@ -74,7 +76,8 @@ struct Worker {
     uint32_t pending_kernels = 0;  // kernels the last enqueued build launched
     unsigned long long *pending_err = nullptr;  // host view of the error words of the last build
     uint64_t timeout_ms = 120000;
-    uint32_t search_group = 0;  // phobic_tuning::search_group (0 = automatic)
+    uint32_t search_group = 0;     // phobic_tuning::search_group (0 = automatic)
+    uint32_t search_pipeline = 0;  // phobic_tuning::search_pipeline
 
     phobic_status init(int device, std::string *err);
     void destroy();
@@ -149,9 +152,9 @@ phobic_status measure_int_peak(Worker &w, double *ops_per_s, double *ms, std::st
 // cudaFuncAttributes::binaryVersion of the library's kernels on `device` (100 = sm_100).
 phobic_status kernel_binary_version(int device, int *version, std::string *err);
 
-// Warps per partition of the search for a build of `partitions` partitions: the
-// context's setting, else the autotuner's table, else 0 (launch_search's rule).
-uint32_t choose_search_group(const Worker &w, const phobic_params *params, uint32_t partitions);
+// Launch shape of the search for a build of `partitions` partitions: the context's
+// setting, else the autotuner's table, else group 0 (launch_search's rule).
+SearchShape choose_search_shape(const Worker &w, const phobic_params *params, uint32_t partitions);
 // Times the search's launch shapes for a ladder of partition counts at these
 // parameters and writes the fastest per size class to the tuning table at path
 // (NULL or "": $PHOBIC_TUNING_FILE, else tuning.tsv beside the library's lib/).

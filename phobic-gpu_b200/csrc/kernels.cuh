@@ -195,13 +195,20 @@ cudaError_t launch_partition(int kind, const MapArgs &a, const PartArgs &p, int 
 // wait on predecessors that never publish: the bounded wait must end in
 // PHOBIC_ERR_TIMEOUT (failure-detection tests).
 cudaError_t launch_scan_stalled(const ScanArgs &a, uint32_t skip, cudaStream_t st);
-// K4.  group = warps searching one partition together (k-split groups, 2 or 4), 1 = one
-// warp per partition, 0 = chosen from the partition count (search_group_for).
-cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, int group = 0);
-// Default group size when the autotuner's table has no line for a build: 4 warps per
-// partition up to 512 partitions, 2 up to 1024, else 1, each only while the groups fit one
-// wave of the group kernel.
-int search_group_for(uint32_t partitions, int sm_count);
+// Launch shape of K4: warps that search one partition together (1, or groups of 2, 4, 8;
+// 0 = chosen from the partition count by search_shape_for) and, for a group, whether it
+// searches several small buckets at once (bucket pipeline) or several pilot counters of one
+// bucket (k-split).
+struct SearchShape {
+    int group = 0;
+    bool pipeline = false;
+};
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, SearchShape shape = SearchShape{});
+// Default shape when the autotuner's table has no line for a build, fitted to the B200's
+// measurements: bucket pipelines of 8 warps up to 256 partitions, of 4 up to 512, of 2 up
+// to 1024, else one warp per partition; a group only while the groups fit one wave of the
+// group kernel.
+SearchShape search_shape_for(uint32_t partitions, int sm_count);
 size_t search_group_smem(uint32_t buckets, uint32_t cap, int W);
 // First failed bounds check of each kernel file in the checked build (source line, 0 =
 // none; always 0 in the normal build); reset clears it.

@@ -651,8 +651,12 @@ __device__ __forceinline__ void group_bar(uint32_t id, uint32_t threads) {
 __host__ __device__ __forceinline__ size_t group_extra_words(uint32_t cap) {
     return ((size_t)kHsWords + scr_words(cap) + 3) & ~size_t(3);
 }
-// Exchange words: [2 parities][W] outcomes, then the job and status words (padded).
-__host__ __device__ __forceinline__ size_t group_xch_words(int W) { return ((size_t)2 * W + 4 + 3) & ~size_t(3); }
+// Exchange words: [2 parities][W] outcomes, the control words (job, nonempty, committed,
+// status), and the bucket pipeline's results: [W] (code << 24 | k, offset) pairs and [W][32]
+// slots (padded).
+__host__ __device__ __forceinline__ size_t group_xch_words(int W) {
+    return ((size_t)2 * W + 4 + 2 * (size_t)W + 32 * (size_t)W + 3) & ~size_t(3);
+}
 __host__ __device__ __forceinline__ size_t group_words(uint32_t B, uint32_t cap, int W) {
     return warp_words(B, cap) + (size_t)(W - 1) * group_extra_words(cap) + group_xch_words(W);
 }
@@ -754,7 +758,16 @@ __device__ __forceinline__ void mark_bucket(const WarpSmem &ws, uint2 L, const u
 // warps then search its buckets in k-split steps.
 // Small builds leave most SMs idle, so the group kernel is not held to the one-warp
 // kernel's 4 CTAs per SM (64 registers): 2 CTAs per SM keep it free of spills.
-template <int W>
+// Bucket pipeline (PIPE): for buckets of at most 32 keys (the tail of the search order),
+// warp w searches bucket j + w completely (smallest k, then smallest o) on the bitmap as it
+// stands, without marking.  Warp 0 then commits the W results in order: a result is kept
+// while its slots are still free after the results before it were marked.  That keeps the
+// sequential answer: the bitmap only gains occupied slots, so a (k, o) valid on the later
+// state was valid on the earlier one, and the smallest valid pair on the earlier state, if
+// still valid, is the smallest on the later one.  A pilot limit or duplicate keys found on the
+// earlier state hold on the later one too.  The first result that conflicts is searched again
+// in the next step.
+template <int W, bool PIPE>
 __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArgs a) {
     extern __shared__ __align__(16) uint32_t smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -767,7 +780,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
         ws.scr = ws.hs + kHsWords;
     }
     uint32_t *xch = gbase + warp_words(a.buckets, a.cap) + (size_t)(W - 1) * group_extra_words(a.cap);
-    uint32_t *ctl = xch + 2 * W;  // [0] job, [1] status / nonempty
+    uint32_t *ctl = xch + 2 * W;  // [0] job, [1] nonempty, [2] committed, [3] status
+    uint32_t *pres = ctl + 4;     // [W] pairs: code << 24 | k, offset
+    uint32_t *pslots = pres + 2 * W;  // [W][32] slots of each warp's result
     uint32_t par = 0;
     for (;;) {
         if (w == 0 && lane == 0) ctl[0] = atomicAdd(a.queue, 1u);
@@ -814,6 +829,65 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
                 const uint32_t b = sc >> 16, st = sc & 0xFFFFu;
                 const uint32_t s = half_get(ws.cnt32, b);
                 const uint2 *src = so + st;
+                if (PIPE && s <= 32) {  // every later bucket is as small (search order: size descending)
+                    const uint32_t jw = j + w;
+                    if (jw < nonempty) {
+                        const uint32_t scw = ws.sched[jw];
+                        const uint32_t sw = half_get(ws.cnt32, scw >> 16);
+                        const uint2 Lw = lane < (int)sw ? so[(scw & 0xFFFFu) + lane] : make_uint2(0, 0);
+                        uint32_t code = kTryLimit, kk = 0, o = 0;
+                        for (uint32_t k = 0; k < k_lim; k++) {
+                            if (k == kDupCheckAt && sw > 1 && has_duplicate_key(Lw, sw, lane)) {
+                                code = kTryDup;
+                                break;
+                            }
+                            if (try_small(ws, Lw, sw, ps, fm, k, rounds, lane, &o) == kTryFound) {
+                                code = kTryFound;
+                                kk = k;
+                                break;
+                            }
+                        }
+                        if (lane == 0) {
+                            pres[2 * w] = (code << 24) | (kk & 0xFFFFFFu);
+                            pres[2 * w + 1] = o;
+                        }
+                        if (code == kTryFound && lane < (int)sw) {
+                            uint32_t q = fm.mod(pilot_hash(Lw.x, Lw.y, kk)) + o;
+                            pslots[32 * w + lane] = q >= ps ? q - ps : q;
+                        }
+                    }
+                    group_bar(bar_id, bar_n);
+                    if (w == 0) {
+                        uint32_t committed = 0, e = PHOBIC_OK;
+                        for (uint32_t v = 0; v < (uint32_t)W && j + v < nonempty; v++) {
+                            const uint32_t r0 = pres[2 * v], rcode = r0 >> 24;
+                            if (rcode != kTryFound) {
+                                e = rcode == kTryDup ? PHOBIC_ERR_DUPLICATE_KEY : PHOBIC_ERR_SEARCH_LIMIT;
+                                break;
+                            }
+                            const uint32_t scv = ws.sched[j + v], bv = scv >> 16;
+                            const uint32_t sv = half_get(ws.cnt32, bv);
+                            const bool mine = lane < (int)sv;
+                            const uint32_t q = mine ? pslots[32 * v + lane] : 0u;
+                            const bool taken = mine && PHB_CHECK(q < ps) && ((ws.occ[q >> 5] >> (q & 31)) & 1u);
+                            if (__any_sync(kFullMask, taken)) break;  // searched again in the next step
+                            mark_if(ws.occ, q, ps, mine && PHB_CHECK(!mine || q < ps));
+                            __syncwarp();
+                            if (lane == 0 && PHB_CHECK(bv < a.buckets))
+                                pil[(size_t)bv * pstride] = pres[2 * v + 1] + ps * (r0 & 0xFFFFFFu);
+                            committed++;
+                        }
+                        if (lane == 0) {
+                            ctl[2] = committed;
+                            ctl[3] = e;
+                        }
+                    }
+                    group_bar(bar_id, bar_n);
+                    err = ctl[3];
+                    j += ctl[2];
+                    j--;  // the loop's increment
+                    continue;
+                }
                 const uint2 L = lane < (int)s && s <= 32 ? src[lane] : make_uint2(0, 0);
                 for (uint32_t k0 = 0;; k0 += W) {
                     const uint32_t k = k0 + w;
@@ -888,40 +962,50 @@ __global__ void __launch_bounds__(kSearchWarps * 32, kSearchCtasPerSm) k_search(
 
 size_t search_group_smem(uint32_t buckets, uint32_t cap, int W) { return 4 * group_words(buckets, cap, W); }
 
-template <int W>
+template <int W, bool PIPE>
 static cudaError_t launch_group(const SearchArgs &a, int sm_count, cudaStream_t st) {
     constexpr int groups = kSearchWarps / W;
     const size_t smem = (size_t)groups * search_group_smem(a.buckets, a.cap, W);
     if (smem > kSearchSmemLimit) return cudaErrorInvalidValue;
-    cudaError_t e = allow_dynamic_smem(k_search_group<W>, smem);
+    cudaError_t e = allow_dynamic_smem(k_search_group<W, PIPE>, smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search_group<W>, kSearchWarps * 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_search_group<W, PIPE>, kSearchWarps * 32, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const uint64_t want = (a.M + groups - 1) / groups;
     const int grid = (int)std::min<uint64_t>(want, (uint64_t)per_sm * sm_count);
-    k_search_group<W><<<grid, kSearchWarps * 32, smem, st>>>(a);
+    k_search_group<W, PIPE><<<grid, kSearchWarps * 32, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-int search_group_for(uint32_t partitions, int sm_count) {
-    // Measured on a B200 (the autotuner's ladder, three key sets per size): groups of 4 are
-    // fastest up to about 256 partitions and protect against retry-heavy partitions (a small
-    // build lasts as long as its slowest one), groups of 2 around 1024, one warp beyond.  A
-    // group must fit one wave of the group kernel (2 CTAs of kSearchWarps warps per SM).
-    const uint64_t sms = (uint64_t)(sm_count > 0 ? sm_count : 148);
-    const uint64_t wave = sms * 2 * kSearchWarps;  // warps of one wave of the group kernel
-    if ((uint64_t)partitions * 4 <= wave && partitions <= 512) return 4;
-    if ((uint64_t)partitions * 2 <= wave && partitions <= 1024) return 2;
-    return 1;
+SearchShape search_shape_for(uint32_t partitions, int sm_count) {
+    // Measured on a B200 (the autotuner's ladder, three key sets per size, six parameter
+    // sets): bucket pipelines of 8 warps are fastest up to 256 partitions, of 4 warps up to
+    // 512, of 2 warps up to 1024; one warp per partition beyond.  A group must fit one wave
+    // of the group kernel (2 CTAs of kSearchWarps warps per SM).
+    const uint64_t wave = (uint64_t)(sm_count > 0 ? sm_count : 148) * 2 * kSearchWarps;
+    SearchShape sh;
+    sh.group = 1;
+    if ((uint64_t)partitions * 8 <= wave && partitions <= 256) sh = SearchShape{8, true};
+    else if ((uint64_t)partitions * 4 <= wave && partitions <= 512) sh = SearchShape{4, true};
+    else if ((uint64_t)partitions * 2 <= wave && partitions <= 1024) sh = SearchShape{2, true};
+    return sh;
 }
 
-cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, int group) {
+cudaError_t launch_search(const SearchArgs &a, int sm_count, cudaStream_t st, SearchShape shape) {
     if (a.M == 0) return cudaSuccess;
-    if (group == 0) group = search_group_for(a.M, sm_count);
-    if (group == 2 || group == 4) {
-        cudaError_t e = group == 2 ? launch_group<2>(a, sm_count, st) : launch_group<4>(a, sm_count, st);
+    if (shape.group == 0) shape = search_shape_for(a.M, sm_count);
+    const int group = shape.group;
+    const bool pipeline = shape.pipeline;
+    if (group == 2 || group == 4 || group == 8) {
+        cudaError_t e;
+        if (pipeline)
+            e = group == 2 ? launch_group<2, true>(a, sm_count, st)
+                : group == 4 ? launch_group<4, true>(a, sm_count, st) : launch_group<8, true>(a, sm_count, st);
+        else
+            e = group == 2 ? launch_group<2, false>(a, sm_count, st)
+                : group == 4 ? launch_group<4, false>(a, sm_count, st) : launch_group<8, false>(a, sm_count, st);
         if (e != cudaErrorInvalidValue) return e;
         cudaGetLastError();  // the group's tables do not fit: one warp per partition
     }

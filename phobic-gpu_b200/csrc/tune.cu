@@ -2,18 +2,20 @@
 //
 // The reference fixes its launch shapes per pipeline as specialisation constants
 // (src/search_stage.cpp:36-37, include/phobicGpu/mphf_builder.h:39-45).  Here the
-// shape that matters across workload sizes is the number of warps searching one
-// partition together (each warp trying its own pilot counter per step, so also the
-// pilots tried per probe): one warp per partition when the partitions fill the GPU,
-// groups of 2 or 4 when a build has few partitions and each partition's search is
-// bound by the latency of its sequential tries.
+// shape that matters across workload sizes is how many warps search one partition
+// together and how: one warp per partition when the partitions fill the GPU; for builds
+// of few partitions, whose search is bound by the latency of each partition's chain of
+// tries, a group of 2, 4 or 8 warps that either tries several pilot counters of one
+// bucket per step (k-split: pilots per probe) or searches several small buckets at once
+// and commits them in order (bucket pipeline).
 //
 // phobic_autotune times every shape on synthetic keys (splitmix64 on the device; three key
 // sets per size, the mean of their best-of-three build times) for a ladder of partition
 // counts at the caller's parameters, and records the fastest
 // per (device name, P, B, partition capacity, size class) as one line of a tab-
 // separated table:
-//     device  partition_size  buckets  max_partition_size  max_partitions  search_group  [ms per shape...]
+//     device  partition_size  buckets  max_partition_size  max_partitions  search_group
+//     search_pipeline  [build ms of each shape of kShapes...]
 // A build looks its shape up in that table (the first line of its device and
 // parameters whose max_partitions is >= its partition count); builds larger than
 // every class, or without a line, use the partition-count rule of launch_search.
@@ -39,7 +41,7 @@ namespace {
 
 struct TuneLine {
     std::string device;
-    uint32_t P, B, cap, max_parts, group;
+    uint32_t P, B, cap, max_parts, group, pipeline;
 };
 
 std::mutex g_tune_mu;
@@ -70,7 +72,7 @@ std::vector<TuneLine> parse_lines(std::istream &f) {
         std::stringstream ss(line);
         std::string c;
         while (std::getline(ss, c, '\t')) col.push_back(c);
-        if (col.size() < 6) continue;
+        if (col.size() < 7) continue;
         TuneLine t;
         t.device = col[0];
         t.P = (uint32_t)std::strtoul(col[1].c_str(), nullptr, 10);
@@ -78,7 +80,9 @@ std::vector<TuneLine> parse_lines(std::istream &f) {
         t.cap = (uint32_t)std::strtoul(col[3].c_str(), nullptr, 10);
         t.max_parts = (uint32_t)std::strtoul(col[4].c_str(), nullptr, 10);
         t.group = (uint32_t)std::strtoul(col[5].c_str(), nullptr, 10);
-        if (t.group == 1 || t.group == 2 || t.group == 4) out.push_back(t);
+        t.pipeline = (uint32_t)std::strtoul(col[6].c_str(), nullptr, 10);
+        const bool ok_group = t.group == 1 || t.group == 2 || t.group == 4 || t.group == 8;
+        if (ok_group && t.pipeline <= 1) out.push_back(t);
     }
     return out;
 }
@@ -119,26 +123,30 @@ std::string device_name(int device) {
 // Size classes of the ladder: partition counts.
 constexpr uint32_t kClasses[] = {16, 64, 256, 512, 768, 1024, 2048, 4096};
 constexpr uint32_t kTuneKeySets = 3;  // key sets timed per class and shape
+// The shapes the autotuner times: one warp; k-split groups of 2 and 4; bucket pipelines of
+// 2, 4 and 8 warps.
+constexpr SearchShape kShapes[] = {{1, false}, {2, false}, {4, false}, {2, true}, {4, true}, {8, true}};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
 }  // namespace
 
-uint32_t choose_search_group(const Worker &w, const phobic_params *params, uint32_t partitions) {
-    if (w.search_group) return w.search_group;
+SearchShape choose_search_shape(const Worker &w, const phobic_params *params, uint32_t partitions) {
+    if (w.search_group) return SearchShape{(int)w.search_group, w.search_pipeline != 0};
     std::lock_guard<std::mutex> lk(g_tune_mu);
     if (!g_tune_loaded) {
         g_tune = parse_table(default_table_path());
         g_tune_loaded = true;
     }
-    if (g_tune.empty()) return 0;
+    if (g_tune.empty()) return SearchShape{};
     const std::string dev = device_name(w.device);
     uint32_t cap = 0, kmax = 0;
-    if (check_params(params, &cap, &kmax, nullptr) != PHOBIC_OK) return 0;
+    if (check_params(params, &cap, &kmax, nullptr) != PHOBIC_OK) return SearchShape{};
     const TuneLine *best = nullptr;
     for (const auto &t : g_tune)
         if (t.device == dev && t.P == params->partition_size && t.B == params->buckets && t.cap == cap &&
             t.max_parts >= partitions && (!best || t.max_parts < best->max_parts))
             best = &t;
-    return best ? best->group : 0;
+    return best ? SearchShape{(int)best->group, best->pipeline != 0} : SearchShape{};
 }
 
 phobic_status autotune(Worker &w, const phobic_params *params, const char *path, uint32_t *lines_written,
@@ -165,10 +173,8 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
         if (err) *err = "autotune: no device memory for the synthetic keys";
         return PHOBIC_ERR_OOM;
     }
-    const uint32_t saved = w.search_group;
-    std::vector<TuneLine> found;
+    const uint32_t saved = w.search_group, saved_pipe = w.search_pipeline;
     std::vector<std::string> rows;
-    const uint32_t shapes[] = {1, 2, 4};
     for (uint32_t ci = 0; ci < sizeof(kClasses) / sizeof(kClasses[0]) && st == PHOBIC_OK; ci++) {
         const uint32_t parts = kClasses[ci];
         const uint64_t n = (uint64_t)parts * P;
@@ -176,14 +182,15 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
         phobic_result r{1, pil, off};
         // A small build lasts as long as its slowest partition, which varies with the keys:
         // each shape is timed on kTuneKeySets key sets and scored by the sum of their times.
-        double ms[3] = {0, 0, 0};
+        double ms[kNumShapes] = {};
         for (uint32_t ks = 0; ks < kTuneKeySets && st == PHOBIC_OK; ks++) {
             if (launch_splitmix(keys, n, 0x7475ull + 97 * ci + 7919 * ks, w.stream) != cudaSuccess) {
                 st = cuda_status(cudaGetLastError(), "autotune keys", err);
                 break;
             }
-            for (int si = 0; si < 3 && st == PHOBIC_OK; si++) {
-                w.search_group = shapes[si];
+            for (int si = 0; si < kNumShapes && st == PHOBIC_OK; si++) {
+                w.search_group = (uint32_t)kShapes[si].group;
+                w.search_pipeline = kShapes[si].pipeline ? 1u : 0u;
                 double best = 1e30;
                 for (int rep = 0; rep < 4 && st == PHOBIC_OK; rep++) {  // one warm-up, best of three
                     phobic_timings t{};
@@ -195,14 +202,19 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
             }
         }
         if (st != PHOBIC_OK) break;
-        const int win = (int)(std::min_element(ms, ms + 3) - ms);
-        found.push_back(TuneLine{dev, P, B, cap, parts, shapes[win]});
-        char row[512];
-        std::snprintf(row, sizeof(row), "%s\t%u\t%u\t%u\t%u\t%u\t%.4f\t%.4f\t%.4f", dev.c_str(), P, B, cap, parts,
-                      shapes[win], ms[0], ms[1], ms[2]);
+        const int win = (int)(std::min_element(ms, ms + kNumShapes) - ms);
+        std::string row = dev + "\t" + std::to_string(P) + "\t" + std::to_string(B) + "\t" + std::to_string(cap) + "\t" +
+                          std::to_string(parts) + "\t" + std::to_string(kShapes[win].group) + "\t" +
+                          (kShapes[win].pipeline ? "1" : "0");
+        for (int si = 0; si < kNumShapes; si++) {
+            char t[32];
+            std::snprintf(t, sizeof(t), "\t%.4f", ms[si]);
+            row += t;
+        }
         rows.push_back(row);
     }
     w.search_group = saved;
+    w.search_pipeline = saved_pipe;
     cleanup();
     if (st != PHOBIC_OK) return st;
     const std::string out_path = path && *path ? std::string(path) : default_table_path();
@@ -224,8 +236,8 @@ phobic_status autotune(Worker &w, const phobic_params *params, const char *path,
         if (err) *err = "autotune: cannot write " + tmp_path;
         return PHOBIC_ERR_INVALID;
     }
-    o << "# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group"
-         "\tbuild_ms_group1\tbuild_ms_group2\tbuild_ms_group4\n";
+    o << "# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group\tsearch_pipeline"
+         "\tbuild_ms_1\tbuild_ms_2k\tbuild_ms_4k\tbuild_ms_2p\tbuild_ms_4p\tbuild_ms_8p\n";
     for (const auto &l : keep) o << l << "\n";
     for (const auto &l : rows) o << l << "\n";
     o.close();

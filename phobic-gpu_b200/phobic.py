@@ -75,7 +75,7 @@ class Timings(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("search_group", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+    _fields_ = [("search_group", C.c_uint32), ("search_pipeline", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 class ServerConfig(C.Structure):
@@ -388,10 +388,12 @@ class Context:
         check(_lib().phobic_debug_stalled_wait(self.handle, wait_ms, C.byref(st)), self)
         return int(st.value)
 
-    def set_tuning(self, search_group: int = 0) -> None:
-        """Launch shapes of later builds: warps per partition of the search (0 = automatic)."""
+    def set_tuning(self, search_group: int = 0, search_pipeline: int = 0) -> None:
+        """Launch shapes of later builds: warps per partition of the search (0 = automatic) and
+        whether a group pipelines small buckets (1) or splits pilot counters (0)."""
         t = Tuning()
         t.search_group = search_group
+        t.search_pipeline = search_pipeline
         check(_lib().phobic_ctx_set_tuning(self.handle, C.byref(t)), self)
 
     def autotune(self, cfg: "MPHFconfig", path: str | None = None) -> int:

@@ -4,10 +4,10 @@
 
 For each case (the parameter sets and set sizes of the benchmark workloads) and seed,
 builds the same synthetic u64 keys (splitmix64 on the device) with every shape of the
-search (phobic_tuning::search_group 1, 2, 4, and 0 = automatic), device-resident keys
-and results, and prints one JSON line per case: build and search ms per shape (CUDA
-events on the context's stream) and whether each shape's pilots equal the one-warp
-build's.  Set PHOBIC_TUNING_FILE to a missing path to see the automatic rule instead of
+search (one warp per partition "1", k-split groups "2k" and "4k", bucket pipelines "2p",
+"4p" and "8p", and "auto", the shape a build gets by default), device-resident keys and
+results, and prints one JSON line per case: build and search ms per shape (CUDA events on
+the context's stream) and whether each shape's pilots equal the one-warp build's.  Set PHOBIC_TUNING_FILE to a missing path to see the automatic rule instead of
 the shipped tuning table.
 """
 from __future__ import annotations
@@ -20,6 +20,7 @@ from pathlib import Path
 
 sys.path.insert(0, str(Path(__file__).resolve().parent))
 
+SHAPES = [("1", 1, 0), ("2k", 2, 0), ("4k", 4, 0), ("2p", 2, 1), ("4p", 4, 1), ("8p", 8, 1), ("auto", 0, 0)]
 CASES = [("C1", 5.0, 2048, 1_000_000), ("C5 median request", 7.0, 2048, 700_000),
          ("C4 small set", 6.0, 2048, 10_000), ("C4 mid set", 6.0, 2048, 100_000),
          ("C4 large set", 6.0, 2048, 4_000_000), ("C5 large request", 7.0, 2048, 20_000_000),
@@ -52,8 +53,8 @@ def main() -> None:
         do = torch.empty(parts + 1, dtype=torch.int32, device="cuda")
         row = {"case": name, "seed": seed, "lambda": lam, "P": P, "n": n, "partitions": parts}
         ref = None
-        for g in (1, 2, 4, 0):
-            ctx.set_tuning(search_group=g)
+        for label, g, pipe in SHAPES:
+            ctx.set_tuning(search_group=g, search_pipeline=pipe)
             steps = 20 if n <= 4_000_000 else 5
             for _ in range(3):
                 ctx.build(keys, cfg, out=(dp, do))
@@ -69,8 +70,8 @@ def main() -> None:
             out = dp.clone()
             same = ref is None or bool(torch.equal(out, ref))
             ref = out if ref is None else ref
-            row[f"g{g}"] = {"build_ms": a.elapsed_time(b) / steps, "search_ms": statistics.median(search),
-                            "equal_g1": same}
+            row[label] = {"build_ms": a.elapsed_time(b) / steps, "search_ms": statistics.median(search),
+                          "equal_1": same}
         ctx.set_tuning(search_group=0)
         print(json.dumps(row), flush=True)
         del keys, dp, do, ref

@@ -47,8 +47,8 @@ def main() -> int:
         got = ctx.build((data, offs), cfg)
         want = O.build(O.hash_keys((data, offs), "strings"), 2048, cfg.bucketCountPerPartition, cfg.getFulcs())
         assert np.array_equal(got.pilots, want["pilots"])
-        for group in (1, 2, 4):  # every search shape, on the same keys
-            ctx.set_tuning(search_group=group)
+        for group, pipe in ((1, 0), (2, 0), (4, 0), (8, 0), (2, 1), (4, 1), (8, 1)):  # every search shape
+            ctx.set_tuning(search_group=group, search_pipeline=pipe)
             for lam, P, n in ((5.0, 2048, 1_000_000), (8.0, 8192, 200_000), (7.5, 4096, 300_000), (3.0, 64, 5000)):
                 g_cfg = phobic.MPHFconfig(lam, P)
                 keys = keygen.splitmix64(700 + n % 1000, n)

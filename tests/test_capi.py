@@ -111,19 +111,20 @@ def test_context_without_device_fails_loudly(phobic):
 
 def test_shipped_tuning_table_is_well_formed(phobic):
     """phobic-gpu_b200/tuning.tsv (written by phobic_autotune on a B200): tab-separated lines
-    of device, P, B, partition capacity, size class, search shape and the three measured
-    build times; for every parameter set the classes ascend and the chosen shape is the
-    fastest measured one."""
+    of device, P, B, partition capacity, size class, search shape (warps, bucket pipeline)
+    and the measured build times of the six timed shapes; for every parameter set the
+    classes ascend and the chosen shape is the fastest measured one."""
+    shapes = [(1, 0), (2, 0), (4, 0), (2, 1), (4, 1), (8, 1)]
     table = ROOT / "phobic-gpu_b200" / "tuning.tsv"
     rows = [l.split("\t") for l in table.read_text().splitlines() if l and not l.startswith("#")]
     assert rows
     groups = {}
     for r in rows:
-        assert len(r) == 9, r
-        dev, P, B, cap, cls, shape = r[0], *map(int, r[1:6])
-        ms = [float(x) for x in r[6:9]]
-        assert shape in (1, 2, 4)
-        assert ms[[1, 2, 4].index(shape)] == min(ms), r
+        assert len(r) == 7 + len(shapes), r
+        dev, P, B, cap, cls, group, pipe = r[0], *map(int, r[1:7])
+        ms = [float(x) for x in r[7:]]
+        assert (group, pipe) in shapes
+        assert ms[shapes.index((group, pipe))] == min(ms), r
         cfg = None
         for lam in (4.5, 5.0, 6.0, 7.0, 7.5):
             c = phobic.MPHFconfig(lam, P)

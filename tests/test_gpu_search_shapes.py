@@ -1,7 +1,8 @@
 """Launch shapes of the search and the autotuner, through the C ABI.
 
-Every shape of the search (one warp per partition, or groups of 2 or 4 warps that
-each try their own pilot counter per step) must give the oracle's pilots bit for bit
+Every shape of the search (one warp per partition; groups of 2, 4 or 8 warps that each
+try their own pilot counter per step; groups that search several small buckets at once
+and commit them in order) must give the oracle's pilots bit for bit
 (search.comp:105-124: smallest pilot counter, then smallest offset), and the same
 error status where the oracle reports one.  The autotuner writes its table and later
 builds still match the oracle."""
@@ -13,7 +14,8 @@ import oracle_lib as O
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [1, 2, 4]
+# (warps per partition, bucket pipeline): one warp; k-split groups; bucket pipelines.
+SHAPES = [(1, 0), (2, 0), (4, 0), (8, 0), (2, 1), (4, 1), (8, 1)]
 
 
 def oracle(keys4, cfg, **kw):
@@ -25,11 +27,12 @@ def oracle(keys4, cfg, **kw):
                                      (8.0, 8192, 200_000), (2.0, 256, 40_000), (1.5, 777, 100_000),
                                      (7.0, 2500, 1), (5.0, 2048, 0), (3.0, 64, 5000)])
 def test_every_search_shape_matches_oracle(phobic, lam, P, n, group):
+    group, pipe = group
     cfg = phobic.MPHFconfig(lam, P)
     keys = keygen.splitmix64(700 + n % 1000, n)
     want = oracle(O.hash_keys(keys, "u64"), cfg)
     with phobic.Context(0) as ctx:
-        ctx.set_tuning(search_group=group)
+        ctx.set_tuning(search_group=group, search_pipeline=pipe)
         if want["status"] != 0:
             with pytest.raises(phobic.PhobicError) as e:
                 ctx.build(keys, cfg)
@@ -44,12 +47,13 @@ def test_every_search_shape_matches_oracle(phobic, lam, P, n, group):
 
 @pytest.mark.parametrize("group", SHAPES)
 def test_search_shapes_strings_pairs_and_batches(phobic, group):
+    group, pipe = group
     cfg = phobic.MPHFconfig(6.0, 2048)
     strs = keygen.strings(41, 30_000)
     pairs = keygen.splitmix64(42, 2 * 25_000).reshape(25_000, 2)
     sets = [keygen.splitmix64(43 + i, 500 * (i + 1) ** 2) for i in range(10)]
     with phobic.Context(0) as ctx:
-        ctx.set_tuning(search_group=group)
+        ctx.set_tuning(search_group=group, search_pipeline=pipe)
         got = ctx.build(strs, cfg)
         assert (got.pilots == oracle(O.hash_keys(strs, "strings"), cfg)["pilots"]).all()
         got = ctx.build(pairs, cfg, kind=phobic.KEYS_BYTES16)
@@ -63,12 +67,13 @@ def test_search_shapes_strings_pairs_and_batches(phobic, group):
 
 @pytest.mark.parametrize("group", SHAPES)
 def test_search_shapes_report_errors_like_the_oracle(phobic, group):
+    group, pipe = group
     cfg = phobic.MPHFconfig(5.0, 2048)
     dup = keygen.splitmix64(1, 3000)
     dup[1] = dup[0]
     limited = keygen.splitmix64(1, 4000)
     with phobic.Context(0) as ctx:
-        ctx.set_tuning(search_group=group)
+        ctx.set_tuning(search_group=group, search_pipeline=pipe)
         with pytest.raises(phobic.PhobicError) as e:
             ctx.build(dup, cfg)
         assert e.value.status == oracle(O.hash_keys(dup, "u64"), cfg)["status"] == phobic.ERR_DUPLICATE_KEY
@@ -91,15 +96,17 @@ def test_search_shapes_report_errors_like_the_oracle(phobic, group):
 def test_autotune_writes_its_table_and_builds_still_match(phobic, tmp_path):
     cfg = phobic.MPHFconfig(5.0, 2048)
     table = tmp_path / "tuning.tsv"
-    table.write_text("# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group\n"
-                     "Some Other GPU\t2048\t410\t3072\t64\t2\n")
+    table.write_text("# device\tpartition_size\tbuckets\tmax_partition_size\tmax_partitions\tsearch_group"
+                     "\tsearch_pipeline\n"
+                     "Some Other GPU\t2048\t410\t3072\t64\t2\t0\n")
     with phobic.Context(0) as ctx:
         assert ctx.autotune(cfg, str(table)) == 8
         lines = [l.split("\t") for l in table.read_text().splitlines() if l and not l.startswith("#")]
-        assert ["Some Other GPU", "2048", "410", "3072", "64", "2"] in [l[:6] for l in lines]
+        assert ["Some Other GPU", "2048", "410", "3072", "64", "2", "0"] in [l[:7] for l in lines]
         ours = [l for l in lines if l[0] != "Some Other GPU"]
         assert [int(l[4]) for l in ours] == [16, 64, 256, 512, 768, 1024, 2048, 4096]
-        assert all(l[5] in ("1", "2", "4") and len(l) == 9 for l in ours)
+        assert all((l[5], l[6]) in (("1", "0"), ("2", "0"), ("4", "0"), ("2", "1"), ("4", "1"), ("8", "1"))
+                   and len(l) == 13 for l in ours)
         keys = keygen.splitmix64(9, 1_000_000)
         got = ctx.build(keys, cfg)
         assert (got.pilots == oracle(O.hash_keys(keys, "u64"), cfg)["pilots"]).all()
