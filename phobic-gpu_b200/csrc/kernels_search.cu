@@ -474,6 +474,28 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
 // ws.sched), bucket-ordered keys (in a.sorted), pilot 0 for empty buckets, a clear
 // bitmap and collision scratch.  *nonempty = buckets to search; *skip = true when the
 // partition is not searched here (reported by the size check).  Returns a status.
+// The bucket-ordered copy of a partition's keys is scratch that lives from the preparation
+// to the end of the partition's search.  It is stored with an L2 evict-last policy, so it is
+// still in L2 when the search reads it back, while the inputs that are read once (the lower
+// hash words and the second read of the bucket ids) are loaded as streaming; once the
+// partition is done its 128-byte lines that no other partition shares are discarded from L2
+// without being written back.
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ void st_evict_last(uint2 *p, uint2 v, uint64_t pol) {
+    asm volatile("st.global.L2::cache_hint.v2.u32 [%0], {%1, %2}, %3;" ::"l"(p), "r"(v.x), "r"(v.y), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void discard_partition_copy(const uint2 *so, uint32_t ps, int lane) {
+    const uintptr_t a = ((uintptr_t)so + 127) & ~(uintptr_t)127;
+    const uintptr_t e = ((uintptr_t)(so + ps)) & ~(uintptr_t)127;
+    for (uintptr_t x = a + 128u * (uint32_t)lane; x < e; x += 32u * 128u)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(x) : "memory");
+}
+
 __device__ __forceinline__ uint32_t prep_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
                                                    uint32_t g, uint32_t p, int lane, uint32_t *nonempty_out,
                                                    bool *skip) {
@@ -572,12 +594,14 @@ __device__ __forceinline__ uint32_t prep_partition(const SearchArgs &a, const Wa
     // Keys into bucket order (redistribute_keys.comp:21-53, inside the partition).
     const uint2 *lo = a.lowers + base;
     uint2 *so = a.sorted + base;
+    const uint64_t keep = l2_evict_last_policy();
 #pragma unroll 4
     for (uint32_t i = lane; i < ps; i += 32) {
-        const uint32_t b = min((uint32_t)bk[i], B - 1);
-        if (!PHB_CHECK(b == bk[i])) continue;
+        const uint16_t bi = __ldcs(bk + i);
+        const uint32_t b = min((uint32_t)bi, B - 1);
+        if (!PHB_CHECK(b == bi)) continue;
         const uint32_t pos = half_add(ws.cur32, b);
-        if (PHB_CHECK(pos < ps)) so[pos] = lo[i];
+        if (PHB_CHECK(pos < ps)) st_evict_last(so + pos, __ldcs(lo + i), keep);
     }
     __threadfence_block();
     __syncwarp();
@@ -626,6 +650,8 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
         if (st_code != PHOBIC_OK) return st_code;
         if (lane == 0 && PHB_CHECK(b < B)) pil[(size_t)b * pstride] = pilot;
     }
+    __syncwarp();
+    discard_partition_copy(so, ps, lane);
     return PHOBIC_OK;
 }
 
@@ -922,6 +948,10 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
         }
         // Everyone is done with this partition's tables before warp 0 fetches and prepares the next.
         group_bar(bar_id, bar_n);
+        if (w == 0 && nonempty != 0xFFFFFFFFu) {
+            const uint32_t base = a.G[(size_t)g * a.gstride];
+            discard_partition_copy(a.sorted + base, a.G[(size_t)(g + 1) * a.gstride] - base, lane);
+        }
     }
 }
 
