@@ -99,6 +99,8 @@ typedef struct phobic_timings {
     float result_transfer;    /* device -> host copy of pilots and offsets */
     float total;              /* first event to last event */
     uint32_t kernels;         /* kernels launched by the call */
+    uint32_t graph_replays;   /* builds of the call whose device stages ran as one replayed
+                               * CUDA graph (see phobic_tuning::graphs_off) */
 } phobic_timings;
 
 /* Launch shapes of a context's builds (no counterpart in the reference, whose shapes are
@@ -113,7 +115,15 @@ typedef struct phobic_tuning {
      * committed in order while their slots stay free), 0 = several pilot counters of one
      * bucket (k-split).  Either way the pilots are those of the sequential search. */
     uint32_t search_pipeline;
-    uint32_t reserved[6];
+    /* 0 (default): a build of at most 2048 partitions whose launches are exactly those of the
+     * context's previous build (same sizes, parameters, search shape and device buffers; keys
+     * and results may hold new contents) is captured as a CUDA graph the second time in a row
+     * and replayed as one graph launch from then on; the memsets, kernels, stage events and
+     * status copy of the build are its nodes.  Larger builds, builds with debug outputs and
+     * builds on a stream the caller is capturing launch stage by stage.  1: every build
+     * launches its stages one by one. */
+    uint32_t graphs_off;
+    uint32_t reserved[5];
 } phobic_tuning;
 
 typedef struct phobic_ctx phobic_ctx;

@@ -178,6 +178,7 @@ phobic_status phobic_build_batch(phobic_ctx *ctx, const phobic_keys *sets, uint3
             timings->result_transfer += t.result_transfer;
             timings->total += t.total;
             timings->kernels += t.kernels;
+            timings->graph_replays += t.graph_replays;
         }
         gk.clear(), gr.clear(), gi.clear();
         return st;
@@ -283,9 +284,10 @@ phobic_status phobic_ctx_set_tuning(phobic_ctx *ctx, const phobic_tuning *t) {
     if (t->search_group != 0 && t->search_group != 1 && t->search_group != 2 && t->search_group != 4 &&
         t->search_group != 8)
         return PHOBIC_ERR_INVALID;
-    if (t->search_pipeline > 1) return PHOBIC_ERR_INVALID;
+    if (t->search_pipeline > 1 || t->graphs_off > 1) return PHOBIC_ERR_INVALID;
     ctx->w.search_group = t->search_group;
     ctx->w.search_pipeline = t->search_pipeline;
+    ctx->w.graphs_off = t->graphs_off;
     return PHOBIC_OK;
 }
 

@@ -78,6 +78,14 @@ struct Worker {
     uint64_t timeout_ms = 120000;
     uint32_t search_group = 0;     // phobic_tuning::search_group (0 = automatic)
     uint32_t search_pipeline = 0;  // phobic_tuning::search_pipeline
+    // The device stages of a build (memsets, K1-K4, status copy) as a CUDA graph: a build
+    // whose launches are those of the previous build (same sizes, parameters, search shape
+    // and buffers) is captured the second time in a row and replayed from then on.
+    uint32_t graphs_off = 0;              // phobic_tuning::graphs_off
+    std::vector<uint64_t> graph_key;      // launch identity of the last build
+    cudaGraphExec_t graph_exec = nullptr;  // captured stages of graph_key, if any
+    bool pending_graph = false;           // the last enqueued build replayed graph_exec
+    void drop_graph();
 
     phobic_status init(int device, std::string *err);
     void destroy();

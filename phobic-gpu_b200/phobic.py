@@ -68,6 +68,7 @@ class Timings(C.Structure):
         ("result_transfer", C.c_float),
         ("total", C.c_float),
         ("kernels", C.c_uint32),
+        ("graph_replays", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -75,7 +76,8 @@ class Timings(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("search_group", C.c_uint32), ("search_pipeline", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("search_group", C.c_uint32), ("search_pipeline", C.c_uint32), ("graphs_off", C.c_uint32),
+                ("reserved", C.c_uint32 * 5)]
 
 
 class ServerConfig(C.Structure):
@@ -388,12 +390,15 @@ class Context:
         check(_lib().phobic_debug_stalled_wait(self.handle, wait_ms, C.byref(st)), self)
         return int(st.value)
 
-    def set_tuning(self, search_group: int = 0, search_pipeline: int = 0) -> None:
-        """Launch shapes of later builds: warps per partition of the search (0 = automatic) and
-        whether a group pipelines small buckets (1) or splits pilot counters (0)."""
+    def set_tuning(self, search_group: int = 0, search_pipeline: int = 0, graphs_off: int = 0) -> None:
+        """Launch shapes of later builds: warps per partition of the search (0 = automatic),
+        whether a group pipelines small buckets (1) or splits pilot counters (0), and whether a
+        build that repeats the previous build's launches may replay them as a CUDA graph (0)
+        or always launches its stages one by one (1)."""
         t = Tuning()
         t.search_group = search_group
         t.search_pipeline = search_pipeline
+        t.graphs_off = graphs_off
         check(_lib().phobic_ctx_set_tuning(self.handle, C.byref(t)), self)
 
     def autotune(self, cfg: "MPHFconfig", path: str | None = None) -> int:
