@@ -454,15 +454,19 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     const bool debug = dbg && (dbg->keys4 || dbg->bucket_sizes) && nsets == 1;
     PHB_TRY(cudaSetDevice(w.device), "cudaSetDevice");
 
-    // Host-side set table (pinned): SetDesc[nsets] | key_base[nsets+1] | part_base[nsets+1] | err[nsets].
+    // Host-side set table (pinned): SetDesc[nsets] | key_base[nsets+1] | part_base[nsets+1] |
+    // fulcrums | err[nsets].  Everything before err goes up in one copy to the same layout on
+    // the device.
     const size_t tab_desc = align256(sizeof(SetDesc) * nsets), tab_kb = align256(8 * (nsets + 1)),
-                 tab_pb = align256(8 * (nsets + 1)), tab_err = align256(8 * nsets);
-    PHB_TRY(w.pinned.reserve(tab_desc + tab_kb + tab_pb + tab_err), "pinned table");
+                 tab_pb = align256(8 * (nsets + 1)), tab_fulcs = align256(4 * kFulcrums), tab_err = align256(8 * nsets);
+    const size_t tab_in = tab_desc + tab_kb + tab_pb + tab_fulcs;
+    PHB_TRY(w.pinned.reserve(tab_in + tab_err), "pinned table");
     char *tab = static_cast<char *>(w.pinned.data());
     SetDesc *hdesc = reinterpret_cast<SetDesc *>(tab);
     uint64_t *hkb = reinterpret_cast<uint64_t *>(tab + tab_desc);
     uint32_t *hpb = reinterpret_cast<uint32_t *>(tab + tab_desc + tab_kb);
-    w.pending_err = reinterpret_cast<unsigned long long *>(tab + tab_desc + tab_kb + tab_pb);
+    std::memcpy(tab + tab_desc + tab_kb + tab_pb, params->fulcrums, 4 * kFulcrums);
+    w.pending_err = reinterpret_cast<unsigned long long *>(tab + tab_in);
     w.pending_sets = nsets;
 
     // Host results: pinned destinations are copied to directly, pageable ones through the
@@ -537,10 +541,11 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
     }
     hkb[nsets] = kb;
     hpb[nsets] = pb;
-    uint32_t *d_fulcs = static_cast<uint32_t *>(take(4 * kFulcrums));
-    SetDesc *d_desc = static_cast<SetDesc *>(take(sizeof(SetDesc) * nsets));
-    uint64_t *d_kb = static_cast<uint64_t *>(take(8 * (nsets + 1)));
-    uint32_t *d_pb = static_cast<uint32_t *>(take(8 * (nsets + 1)));
+    char *d_tab = static_cast<char *>(take(tab_in));
+    SetDesc *d_desc = reinterpret_cast<SetDesc *>(d_tab);
+    uint64_t *d_kb = reinterpret_cast<uint64_t *>(d_tab + tab_desc);
+    uint32_t *d_pb = reinterpret_cast<uint32_t *>(d_tab + tab_desc + tab_kb);
+    uint32_t *d_fulcs = reinterpret_cast<uint32_t *>(d_tab + tab_desc + tab_kb + tab_pb);
     unsigned long long *d_err = static_cast<unsigned long long *>(take(8 * nsets));
     uint32_t *d_queue = static_cast<uint32_t *>(take(64));
     const uint64_t MS = M * plan.stride;  // count matrix entries
@@ -561,10 +566,7 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
         if (err) *err = "arena sizing error";
         return PHOBIC_ERR_OOM;
     }
-    PHB_TRY(cudaMemcpyAsync(d_fulcs, params->fulcrums, 4 * kFulcrums, cudaMemcpyHostToDevice, s), "H2D fulcrums");
-    PHB_TRY(cudaMemcpyAsync(d_desc, hdesc, sizeof(SetDesc) * nsets, cudaMemcpyHostToDevice, s), "H2D sets");
-    PHB_TRY(cudaMemcpyAsync(d_kb, hkb, 8 * (nsets + 1), cudaMemcpyHostToDevice, s), "H2D sets");
-    PHB_TRY(cudaMemcpyAsync(d_pb, hpb, 4 * (nsets + 1), cudaMemcpyHostToDevice, s), "H2D sets");
+    PHB_TRY(cudaMemcpyAsync(d_tab, tab, tab_in, cudaMemcpyHostToDevice, s), "H2D set table and fulcrums");
     uint64_t kc_index = 0, kc_mask = 0;
     const bool key_change = nsets == 1 && take_key_change(N, kind, &kc_index, &kc_mask);
     const uint32_t wshift = part_wshift(M);
