@@ -655,8 +655,12 @@ phobic_status enqueue_sets(Worker &w, const phobic_keys *sets, uint32_t nsets, c
             cudaGetLastError();  // a capture that failed leaves nothing enqueued: launch one by one
         }
         if (w.graph_exec) {
-            PHB_TRY(cudaGraphLaunch(w.graph_exec, s), "graph launch");
-            w.pending_graph = true;
+            if (cudaGraphLaunch(w.graph_exec, s) == cudaSuccess) {
+                w.pending_graph = true;
+            } else {  // launched stage by stage below, which reports a lasting error
+                cudaGetLastError();
+                w.drop_graph();
+            }
         }
     }
     if (!w.pending_graph) {
