@@ -313,11 +313,14 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
                                                 uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
     const bool mine = lane < (int)s;
     const uint32_t padded = (s + 3) & ~3u;
+    // Every lane hashes (no divergent branch); lanes past the bucket take distinct
+    // out-of-range values, so they never collide.  The hash of counter k + 1 is formed
+    // while counter k is tested: the two dependency chains overlap.
+    uint32_t hk_next = fm.mod(pilot_hash(L.x, L.y, 0u));
     for (uint32_t k = 0; k < k_lim; k++) {
         if (k == kDupCheckAt && s > 1 && has_duplicate_key(L, s, lane)) return PHOBIC_ERR_DUPLICATE_KEY;
-        // Every lane hashes (no divergent branch); lanes past the bucket take distinct
-        // out-of-range values, so they never collide.
-        const uint32_t hk = fm.mod(pilot_hash(L.x, L.y, k));
+        const uint32_t hk = hk_next;
+        hk_next = fm.mod(pilot_hash(L.x, L.y, k + 1));
         const uint32_t h = mine ? hk : (0x80000000u | lane);
         if (s > 1) {
             uint32_t m = __match_any_sync(kFullMask, h);
