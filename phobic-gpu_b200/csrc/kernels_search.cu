@@ -308,6 +308,50 @@ __device__ __forceinline__ void mark_if(uint32_t *occ, uint32_t q, uint32_t ps, 
         : "memory");
 }
 
+// A bucket of at most S keys (S = 4 or 8) in a partition of at most 3072 slots: the warp
+// hashes 32 / S pilot counters at once (lane t * S + i holds key i under counter k0 + t; lanes
+// past the bucket hold key 0, the padding the scan expects) and tests them in counter order, so
+// a counter that fails costs no new hash or collision test.  Same result as trying
+// k = 0, 1, 2, ... one at a time (search.comp:105-124).
+template <int S>
+__device__ __forceinline__ uint32_t place_batched(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
+                                                  uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
+    constexpr int G = 32 / S;
+    constexpr uint32_t kGroupMask = (1u << S) - 1u;
+    const int t = lane / S, i = lane % S;
+    const bool key = i < (int)s;
+    const uint32_t lx = __shfl_sync(kFullMask, L.x, key ? i : 0), ly = __shfl_sync(kFullMask, L.y, key ? i : 0);
+    const int pick = lane < (int)s ? lane : 0;  // the key whose slot this lane passes to the scan
+    const bool mine = lane < (int)s;
+    for (uint32_t k0 = 0;; k0 += G) {
+        const uint32_t hk = fm.mod(pilot_hash(lx, ly, k0 + (uint32_t)t));
+        // Two keys of one counter on one slot: the counter rides above the slot (slots < 2^16).
+        uint32_t coll = 0;
+        if (s > 1) {
+            const uint32_t v = key ? (hk | ((uint32_t)t << 24)) : (0x80000000u | (uint32_t)lane);
+            const uint32_t m = __match_any_sync(kFullMask, v);
+            coll = __ballot_sync(kFullMask, key && (m & (m - 1)) != 0);
+        }
+        const uint32_t pk = pack_slot(hk);
+#pragma unroll 1
+        for (int u = 0; u < G; u++) {
+            const uint32_t k = k0 + (uint32_t)u;
+            if (k >= k_lim) return PHOBIC_ERR_SEARCH_LIMIT;
+            if (k == kDupCheckAt && s > 1 && has_duplicate_key(L, s, lane)) return PHOBIC_ERR_DUPLICATE_KEY;
+            if ((coll >> (u * S)) & kGroupMask) continue;
+            const uint32_t hp = __shfl_sync(kFullMask, pk, u * S + pick);
+            const uint32_t o = first_free_offset_unr<S>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
+            if (o == kNone) continue;
+            uint32_t q = __shfl_sync(kFullMask, hk, u * S + pick) + o;
+            q = q >= ps ? q - ps : q;
+            mark_if(ws.occ, q, ps, mine && PHB_CHECK(!mine || q < ps));
+            __syncwarp();
+            *pilot = o + ps * k;
+            return PHOBIC_OK;
+        }
+    }
+}
+
 // One bucket of at most 32 keys; key `lane` in L.  Returns a status code.
 __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
                                                 uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
@@ -327,13 +371,8 @@ __device__ __forceinline__ uint32_t place_small(const WarpSmem &ws, uint2 L, uin
             if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) continue;
         }
         const uint32_t hp = pack_slot(__shfl_sync(kFullMask, h, mine ? lane : 0));
-        uint32_t o;
-        if (s <= 8 && rounds <= 3) {
-            // Two unrolled variants only: a smaller hot loop (fewer instruction-cache
-            // misses) outweighs the repeated slot of buckets of one or two keys.
-            if (s <= 4) o = first_free_offset_unr<4>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
-            else o = first_free_offset_unr<8>(ws.occ, hp, ps, rounds, lane, ws.occ_lo, ws.occ_hi);
-        } else if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
+        uint32_t o;  // buckets of at most 8 keys with at most three rounds go to place_batched
+        if (s <= 4) o = first_free_offset_reg<4>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
         else if (s <= 8) o = first_free_offset_reg<8>(ws.occ, hp, ps, lane, ws.occ_lo, ws.occ_hi);
         else {
             if (lane < (int)padded) ws.hs[lane] = hp;
@@ -647,7 +686,9 @@ __device__ __forceinline__ uint32_t search_partition(const SearchArgs &a, const 
             L_next = lane < (int)s_next ? so[(sc_next & 0xFFFFu) + lane] : make_uint2(0, 0);
         }
         uint32_t pilot = 0;
-        const uint32_t st_code = s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
+        const uint32_t st_code = s <= 4 && rounds <= 3 ? place_batched<4>(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
+                                 : s <= 8 && rounds <= 3 ? place_batched<8>(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
+                                 : s <= 32 ? place_small(ws, L, s, ps, fm, k_lim, rounds, lane, &pilot)
                                  : s <= 64  ? place_large_reg<2>(ws, so + st, s, ps, fm, k_lim, lane, &pilot)
                                             : place_large(ws, so + st, s, ps, fm, k_lim, lane, &pilot);
         if (st_code != PHOBIC_OK) return st_code;
