@@ -312,10 +312,14 @@ __device__ __forceinline__ void mark_if(uint32_t *occ, uint32_t q, uint32_t ps, 
 // hashes 32 / S pilot counters at once (lane t * S + i holds key i under counter k0 + t; lanes
 // past the bucket hold key 0, the padding the scan expects) and tests them in counter order, so
 // a counter that fails costs no new hash or collision test.  Same result as trying
-// k = 0, 1, 2, ... one at a time (search.comp:105-124).
-template <int S>
+// k = 0, 1, 2, ... one at a time (search.comp:105-124).  With MARK the slots are marked and
+// *pilot written; without, nothing is marked and the bucket pipeline gets the counter, the
+// offset and (lanes < s) the lane's slot in *k_out, *o_out, *q_out.
+template <int S, bool MARK = true>
 __device__ __forceinline__ uint32_t place_batched(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
-                                                  uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot) {
+                                                  uint32_t k_lim, uint32_t rounds, int lane, uint32_t *pilot,
+                                                  uint32_t *k_out = nullptr, uint32_t *o_out = nullptr,
+                                                  uint32_t *q_out = nullptr) {
     constexpr int G = 32 / S;
     constexpr uint32_t kGroupMask = (1u << S) - 1u;
     const int t = lane / S, i = lane % S;
@@ -344,9 +348,15 @@ __device__ __forceinline__ uint32_t place_batched(const WarpSmem &ws, uint2 L, u
             if (o == kNone) continue;
             uint32_t q = __shfl_sync(kFullMask, hk, u * S + pick) + o;
             q = q >= ps ? q - ps : q;
-            mark_if(ws.occ, q, ps, mine && PHB_CHECK(!mine || q < ps));
-            __syncwarp();
-            *pilot = o + ps * k;
+            if constexpr (MARK) {
+                mark_if(ws.occ, q, ps, mine && PHB_CHECK(!mine || q < ps));
+                __syncwarp();
+                *pilot = o + ps * k;
+            } else {
+                *k_out = k;
+                *o_out = o;
+                *q_out = q;
+            }
             return PHOBIC_OK;
         }
     }
@@ -906,24 +916,36 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
                         const uint32_t sw = half_get(ws.cnt32, scw >> 16);
                         const uint2 Lw = lane < (int)sw ? so[(scw & 0xFFFFu) + lane] : make_uint2(0, 0);
                         uint32_t code = kTryLimit, kk = 0, o = 0;
-                        for (uint32_t k = 0; k < k_lim; k++) {
-                            if (k == kDupCheckAt && sw > 1 && has_duplicate_key(Lw, sw, lane)) {
-                                code = kTryDup;
-                                break;
+                        if (sw <= 8 && rounds <= 3) {  // several counters hashed at once
+                            uint32_t q = 0;
+                            const uint32_t st = sw <= 4 ? place_batched<4, false>(ws, Lw, sw, ps, fm, k_lim, rounds,
+                                                                                  lane, nullptr, &kk, &o, &q)
+                                                        : place_batched<8, false>(ws, Lw, sw, ps, fm, k_lim, rounds,
+                                                                                  lane, nullptr, &kk, &o, &q);
+                            code = st == PHOBIC_OK                  ? kTryFound
+                                   : st == PHOBIC_ERR_DUPLICATE_KEY ? kTryDup
+                                                                    : kTryLimit;
+                            if (code == kTryFound && lane < (int)sw) pslots[32 * w + lane] = q;
+                        } else {
+                            for (uint32_t k = 0; k < k_lim; k++) {
+                                if (k == kDupCheckAt && sw > 1 && has_duplicate_key(Lw, sw, lane)) {
+                                    code = kTryDup;
+                                    break;
+                                }
+                                if (try_small(ws, Lw, sw, ps, fm, k, rounds, lane, &o) == kTryFound) {
+                                    code = kTryFound;
+                                    kk = k;
+                                    break;
+                                }
                             }
-                            if (try_small(ws, Lw, sw, ps, fm, k, rounds, lane, &o) == kTryFound) {
-                                code = kTryFound;
-                                kk = k;
-                                break;
+                            if (code == kTryFound && lane < (int)sw) {
+                                uint32_t q = fm.mod(pilot_hash(Lw.x, Lw.y, kk)) + o;
+                                pslots[32 * w + lane] = q >= ps ? q - ps : q;
                             }
                         }
                         if (lane == 0) {
                             pres[2 * w] = (code << 24) | (kk & 0xFFFFFFu);
                             pres[2 * w + 1] = o;
-                        }
-                        if (code == kTryFound && lane < (int)sw) {
-                            uint32_t q = fm.mod(pilot_hash(Lw.x, Lw.y, kk)) + o;
-                            pslots[32 * w + lane] = q >= ps ? q - ps : q;
                         }
                     }
                     group_bar(bar_id, bar_n);
