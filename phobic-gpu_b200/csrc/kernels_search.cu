@@ -522,10 +522,6 @@ __device__ __forceinline__ uint32_t place_large_reg(const WarpSmem &ws, const ui
     return PHOBIC_ERR_SEARCH_LIMIT;
 }
 
-// Preparation of one partition by one warp: bucket histogram, search order (in
-// ws.sched), bucket-ordered keys (in a.sorted), pilot 0 for empty buckets, a clear
-// bitmap and collision scratch.  *nonempty = buckets to search; *skip = true when the
-// partition is not searched here (reported by the size check).  Returns a status.
 // The bucket-ordered copy of a partition's keys is scratch that lives from the preparation
 // to the end of the partition's search.  It is stored with an L2 evict-last policy, so it is
 // still in L2 when the search reads it back, while the inputs that are read once (the lower
@@ -548,6 +544,10 @@ __device__ __forceinline__ void discard_partition_copy(const uint2 *so, uint32_t
         asm volatile("discard.global.L2 [%0], 128;" ::"l"(x) : "memory");
 }
 
+// Preparation of one partition by one warp: bucket histogram, search order (in
+// ws.sched), bucket-ordered keys (in a.sorted), pilot 0 for empty buckets, a clear
+// bitmap and collision scratch.  *nonempty = buckets to search; *skip = true when the
+// partition is not searched here (reported by the size check).  Returns a status.
 __device__ __forceinline__ uint32_t prep_partition(const SearchArgs &a, const WarpSmem &ws, const SetDesc &d,
                                                    uint32_t g, uint32_t p, int lane, uint32_t *nonempty_out,
                                                    bool *skip) {
