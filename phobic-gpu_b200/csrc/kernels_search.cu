@@ -741,13 +741,14 @@ __host__ __device__ __forceinline__ size_t group_words(uint32_t B, uint32_t cap,
     return warp_words(B, cap) + (size_t)(W - 1) * group_extra_words(cap) + group_xch_words(W);
 }
 
-// One try of pilot counter k for a bucket of s <= 32 keys (key `lane` in L): the
-// collision test and offset scan of place_small.  kTryFound with *o, else kTryNone.
-__device__ __forceinline__ uint32_t try_small(const WarpSmem &ws, uint2 L, uint32_t s, uint32_t ps, FastMod fm,
-                                              uint32_t k, uint32_t rounds, int lane, uint32_t *o_out) {
+// One try of a pilot counter for a bucket of s <= 32 keys, hk holding key `lane`'s slot
+// under that counter: the collision test and offset scan of place_small.  kTryFound with
+// *o, else kTryNone.
+__device__ __forceinline__ uint32_t try_small(const WarpSmem &ws, uint32_t s, uint32_t ps, uint32_t hk,
+                                              uint32_t rounds, int lane, uint32_t *o_out) {
     const bool mine = lane < (int)s;
     const uint32_t padded = (s + 3) & ~3u;
-    const uint32_t h = mine ? fm.mod(pilot_hash(L.x, L.y, k)) : (0x80000000u | lane);
+    const uint32_t h = mine ? hk : (0x80000000u | lane);
     if (s > 1) {
         uint32_t m = __match_any_sync(kFullMask, h);
         if (__any_sync(kFullMask, mine && (m & (m - 1)) != 0)) return kTryNone;
@@ -927,19 +928,23 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
                                                                     : kTryLimit;
                             if (code == kTryFound && lane < (int)sw) pslots[32 * w + lane] = q;
                         } else {
+                            // The hash of counter k + 1 is formed while counter k is tested.
+                            uint32_t hk_next = fm.mod(pilot_hash(Lw.x, Lw.y, 0u)), hk = 0;
                             for (uint32_t k = 0; k < k_lim; k++) {
                                 if (k == kDupCheckAt && sw > 1 && has_duplicate_key(Lw, sw, lane)) {
                                     code = kTryDup;
                                     break;
                                 }
-                                if (try_small(ws, Lw, sw, ps, fm, k, rounds, lane, &o) == kTryFound) {
+                                hk = hk_next;
+                                hk_next = fm.mod(pilot_hash(Lw.x, Lw.y, k + 1));
+                                if (try_small(ws, sw, ps, hk, rounds, lane, &o) == kTryFound) {
                                     code = kTryFound;
                                     kk = k;
                                     break;
                                 }
                             }
                             if (code == kTryFound && lane < (int)sw) {
-                                uint32_t q = fm.mod(pilot_hash(Lw.x, Lw.y, kk)) + o;
+                                const uint32_t q = hk + o;
                                 pslots[32 * w + lane] = q >= ps ? q - ps : q;
                             }
                         }
@@ -988,7 +993,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 2) k_search_group(SearchArg
                     else if (k == kDupCheckAt && s > 1 &&
                              (s <= 32 ? has_duplicate_key(L, s, lane) : has_duplicate_key_src(src, s, lane)))
                         code = kTryDup;
-                    else code = s <= 32 ? try_small(ws, L, s, ps, fm, k, rounds, lane, &o)
+                    else code = s <= 32 ? try_small(ws, s, ps, fm.mod(pilot_hash(L.x, L.y, k)), rounds, lane, &o)
                                         : try_large(ws, src, s, ps, fm, k, lane, &o);
                     if (lane == 0) xch[par * W + w] = (code << 16) | (o & 0xFFFFu);
                     group_bar(bar_id, bar_n);
